@@ -1,0 +1,406 @@
+#!/usr/bin/env python3
+"""RK3 steps/s of TURBID's flat-channel substep on B200.
+
+Workload (default "cfg3"): 256x256x257 Fourier-Chebyshev grid, oscillatory
+boundary layer Re_delta = 800 with one fine-sediment scalar (Ws = 5e-4,
+Sc = 0.5, Boussinesq coupling s = 2.65, C = 1e-3, erosion/deposition bottom),
+dt = 2 pi/2000, mixed precision (FP32 transforms and nonlinear products, FP64
+z-operators and Helmholtz solves).  Synthetic seeded initial state (the
+reference has no public dataset).  One "step" = one full RK3 step (3 stages
+of both phases).  All fields (>= 300 MB of spectral state plus physical
+buffers) exceed the 126 MB L2, so no explicit L2 flush is done between steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Rank 0 prints one JSON line.  With N > 1 (torchrun) every rank runs an
+independent replica of the case (the path has no cross-case exchange), and
+value = total steps of all ranks / max-over-ranks device time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "RK3 steps/sec @256x256x257, mixed vs FP64 GPU at rel-L2<=1e-5; HBM GB/s"
+
+WORKLOADS = {
+    # name: grid, physics, precision
+    "cfg3": dict(nx=256, ny=256, nz=257, nphase=2, reynolds=800.0, precision="mixed"),
+    "cfg2": dict(nx=128, ny=128, nz=129, nphase=2, reynolds=800.0, precision="fp64"),
+    "cfg1": dict(nx=32, ny=32, nz=65, nphase=1, reynolds=180.0, precision="fp64"),
+    "cfg5": dict(nx=512, ny=256, nz=257, nphase=2, reynolds=1000.0, precision="mixed", lx=8 * math.pi),
+    "small": dict(nx=64, ny=64, nz=65, nphase=2, reynolds=800.0, precision="mixed"),
+}
+
+
+def case_params(name: str) -> dict:
+    w = dict(WORKLOADS[name])
+    p = dict(lx=4 * math.pi, ly=2 * math.pi, dt=2 * math.pi / 2000, froude=1.0, averaged_concentration=1e-3,
+             specific_gravity=2.65, affected_by_scalar=1, bc_u=[1, 0, 0, 1, 0], bc_v=[1, 0, 0, 1, 0],
+             bc_w=[1, 0, 1, 0, 0], bc_p=[0, 1, 0, 1, 0], force_type=2, force_direction=[0, 1],
+             force_amplitude=[0, 1], schmidt=0.5, settling=5e-4, erosion_rate=1e-4, critical_shear=2e-4,
+             scalar_bc=1)
+    if w["nphase"] == 1:
+        p["bc_u"] = p["bc_v"] = [1, 0, 0, 1, 0]
+    p.update(w)
+    return p
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self) -> dict:
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.count(",") >= 8]
+        os.unlink(self.f.name)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                smax = float(r[2])
+            except ValueError:
+                continue
+            for i, n in enumerate(names):
+                if r[5 + i].strip().lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks() -> dict:
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+def fp64_gemm_peak(torch) -> float:
+    """cuBLAS DGEMM TFLOP/s measured in this run (the FP64 tensor-core reference)."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    for _ in range(2):
+        torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 0.0
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        best = max(best, 2 * n ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e12)
+    del a, b
+    torch.cuda.empty_cache()
+    return best
+
+
+def traffic_summary() -> dict:
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the FP64 oracle port of the reference path on the host cores
+# ---------------------------------------------------------------------------
+def cpu_step_rate(wname: str, nsteps_max: int, budget_s: float, warmup: int):
+    from oracle import turbid_oracle as O
+    from turbid_b200 import synthetic
+    p = case_params(wname)
+    keys = [f for f in O.CaseConfig.__dataclass_fields__ if f in p]
+    cfg = O.CaseConfig(**{k: p[k] for k in keys})
+    uvw, pr, phi = synthetic.initial_state(seed=1234, **p)
+    t0 = time.perf_counter()
+    sol = O.OracleSolver(cfg, uvw, pr, phi if cfg.nphase > 1 else None)
+    setup = time.perf_counter() - t0
+    for _ in range(min(warmup, 1)):
+        sol.run_step()
+    done, t0 = 0, time.perf_counter()
+    while done < nsteps_max:
+        sol.run_step()
+        done += 1
+        if time.perf_counter() - t0 > budget_s:
+            break
+    el = time.perf_counter() - t0
+    return done / el, done, el, setup
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    cores = int(os.environ.get("TURBID_ORACLE_THREADS", os.cpu_count() or 1))
+    rate, done, el, setup = cpu_step_rate(args.workload, args.steps, args.cpu_budget, args.warmup)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": rate, "unit": "steps/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / rate, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"{args.workload} " + wdesc(args.workload), "precision": "fp64 (CPU)"},
+        "cpu_baseline": {"value": rate, "unit": "steps/s", "cores": cores, "kind": "port",
+                         "sample": f"{done} RK3 step(s) of the full grid after min(W,1) warm-up step(s), "
+                                   f"{el:.1f} s timed (budget {args.cpu_budget:.0f} s); numpy/scipy FP64 "
+                                   f"restatement of the reference path (the reference needs MPI/Fortran/MKL "
+                                   f"and does not build here)"},
+        "e2e": {"value": rate, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def wdesc(name):
+    p = WORKLOADS[name]
+    return f"{p['nx']}x{p['ny']}x{p['nz']} Re{int(p['reynolds'])} {'+sediment' if p['nphase'] > 1 else ''}"
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def our_arm(args):
+    import torch
+    import turbid_b200 as tb
+    from turbid_b200 import synthetic, _lib
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+    params = case_params(args.workload)
+    prec = args.precision or params["precision"]
+    uvw0, p0, phi0 = synthetic.initial_state(seed=1234, **params)
+    lib = _lib.load()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(v):
+        if dist is None:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    stream = torch.cuda.current_stream()
+    case = tb.ChannelCase(**dict(params, precision=prec))
+    case.set_stream(stream.cuda_stream)
+    case.upload_state(uvw0, p0, phi0)
+    case.run_steps(args.warmup)
+    barrier()
+
+    # ---- device-timed steps (state resident in HBM)
+    sampler = ClockSampler(local) if rank == 0 else None
+    if sampler:
+        sampler.start()
+    l0 = lib.tg_launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    e0.record(stream)
+    done = case.run_steps(args.steps)
+    e1.record(stream)
+    barrier()
+    launches = lib.tg_launch_count() - l0
+    clocks = sampler.stop() if sampler else None
+    ms = max_over_ranks(e0.elapsed_time(e1))
+    total_steps = done * world
+    value = total_steps / (ms * 1e-3)
+
+    # ---- kernel classes of the same workload (separate pass, CUDA events per launch)
+    case.profile_begin()
+    case.run_steps(args.prof_steps)
+    prof = case.profile_end()
+    peaks = measured_peaks()
+
+    # ---- e2e through the C ABI with host buffers: H2D of the restart state,
+    # K steps each returning the 50-double feature vector, D2H of the state
+    pin = {k: torch.from_numpy(v.view(np.float64)).pin_memory() for k, v in
+           (("u", np.ascontiguousarray(uvw0)), ("p", np.ascontiguousarray(p0)), ("c", np.ascontiguousarray(phi0)))}
+    outs = {k: torch.empty_like(v).pin_memory() for k, v in pin.items()}
+    feats = np.zeros(50)
+
+    def ptr(t):
+        import ctypes
+        return ctypes.cast(t.data_ptr(), ctypes.POINTER(ctypes.c_double))
+
+    barrier()
+    t0 = time.perf_counter()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    tb._lib.check(lib.tg_upload_state(case.h, ptr(pin["u"]), ptr(pin["p"]), ptr(pin["c"]), 0))
+    n_e2e = 0
+    for _ in range(args.steps):
+        n_e2e += case.run_steps(1, features=feats)
+    tb._lib.check(lib.tg_download_state(case.h, ptr(outs["u"]), ptr(outs["p"]), ptr(outs["c"])))
+    f1.record(stream)
+    barrier()
+    e2e_ms = max_over_ranks(max(f0.elapsed_time(f1), (time.perf_counter() - t0) * 1e3))
+    state_bytes = sum(v.numel() * 8 for v in pin.values())
+    e2e = {"value": n_e2e * world / (e2e_ms * 1e-3), "unit": "steps/s",
+           "h2d_bytes_per_step": state_bytes / max(n_e2e, 1) + 16,
+           "d2h_bytes_per_step": state_bytes / max(n_e2e, 1) + 400,
+           "what": "tg_upload_state from pinned host (restart layout) + K x tg_run_steps(1) with the 400-byte "
+                   "feature vector read back each step + tg_download_state, all inside the timed region"}
+
+    # ---- accuracy vs the FP64 GPU path + FP64 GPU rate (same seed, same steps)
+    acc = None
+    fp64_rate = None
+    if prec == "mixed" and not args.skip_accuracy:
+        ref = tb.ChannelCase(**dict(params, precision="fp64"))
+        ref.set_stream(stream.cuda_stream)
+        ref.upload_state(uvw0, p0, phi0)
+        ref.run_steps(args.warmup)
+        barrier()
+        g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        g0.record(stream)
+        nd = ref.run_steps(args.steps)
+        g1.record(stream)
+        barrier()
+        fp64_rate = nd / (g0.elapsed_time(g1) * 1e-3)
+        # same initial state, same number of steps in both precisions
+        nacc = args.acc_steps
+        for c in (case, ref):
+            c.upload_state(uvw0, p0, phi0)
+            c.run_steps(nacc)
+        a_u, a_p, a_c = case.download_state()
+        b_u, b_p, b_c = ref.download_state()
+
+        def rl(a, b):
+            return float(np.linalg.norm((a - b).ravel()) / max(np.linalg.norm(b.ravel()), 1e-300))
+        acc = {"steps": nacc, "u": rl(a_u[0], b_u[0]), "v": rl(a_u[1], b_u[1]), "w": rl(a_u[2], b_u[2]),
+               "p": rl(a_p, b_p)}
+        if params["nphase"] > 1:
+            acc["c"] = rl(a_c, b_c)
+        acc["max"] = max(v for k, v in acc.items() if k != "steps")
+        acc["tolerance"] = 1e-5
+        ref.close()
+
+    # ---- roofline of the dominant kernel class
+    steps_p = max(args.prof_steps, 1)
+    dom = max(prof, key=lambda k: prof[k]["ms"])
+    d = prof[dom]
+    traffic = traffic_summary().get(args.workload, {}).get(prec, {}).get(dom)
+    if dom == "zgemm":
+        peak = fp64_gemm_peak(torch)
+        achieved = d["flops"] / (d["ms"] * 1e-3) / 1e12
+        roof = {"kernel": "zgemm64_kernel (FP64 DMMA z-operator GEMM)", "bound": "tensor", "achieved": achieved,
+                "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no FP64 figure)",
+                "per_launch_flops": d["flops"] / max(d["count"], 1), "traffic": traffic}
+    else:
+        peak = peaks.get("hbm_gbs", 6650.0)
+        achieved = d["bytes"] / (d["ms"] * 1e-3) / 1e9
+        roof = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback",
+                "traffic": traffic}
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    kernels = {}
+    for k, v in prof.items():
+        if v["count"] == 0:
+            continue
+        gbs = v["bytes"] / (v["ms"] * 1e-3) / 1e9 if v["ms"] > 0 else 0.0
+        ent = {"ms_per_step": v["ms"] / steps_p, "launches_per_step": v["count"] / steps_p, "GB/s": gbs,
+               "hbm_frac": gbs / hbm}
+        if v["flops"]:
+            ent["TFLOP/s"] = v["flops"] / (v["ms"] * 1e-3) / 1e12
+        kernels[k] = ent
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        try:
+            rate, n, el, setup = cpu_step_rate(args.workload, 1, args.cpu_budget, 0)
+            cpu = {"value": rate, "unit": "steps/s",
+                   "cores": int(os.environ.get("TURBID_ORACLE_THREADS", os.cpu_count() or 1)), "kind": "port",
+                   "sample": f"{n} full RK3 step(s) of the same grid ({el:.1f} s), numpy/scipy FP64 restatement "
+                             f"of the reference path on all host threads"}
+        except Exception as exc:  # the baseline is a report, never a reason to lose the GPU line
+            cpu = {"value": None, "unit": "steps/s", "cores": os.cpu_count(), "kind": "port",
+                   "sample": f"failed: {exc}"}
+    case.close()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / max(done, 1), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 transforms/products + f64 z-solves" if prec == "mixed" else "f64",
+            "data": "synthetic (seeded Stokes profile + divergence-free perturbation, 10% scalar noise)",
+            "config": {"workload": f"{args.workload} {wdesc(args.workload)}", "precision": prec,
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                       "l2": "inputs larger than L2 (no flush)"},
+            "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks, "roofline": roof,
+            "cpu_baseline": cpu, "accuracy_vs_fp64_gpu": acc, "fp64_gpu_steps_per_s": fp64_rate,
+            "kernels": kernels,
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="cfg3", choices=sorted(WORKLOADS))
+    ap.add_argument("--precision", default=None, choices=[None, "fp64", "mixed"])
+    ap.add_argument("--prof-steps", type=int, default=3)
+    ap.add_argument("--acc-steps", type=int, default=100)
+    ap.add_argument("--skip-accuracy", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-budget", type=float, default=60.0)
+    args = ap.parse_args()
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        our_arm(args)
+
+
+if __name__ == "__main__":
+    main()

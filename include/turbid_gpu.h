@@ -1,0 +1,198 @@
+/*
+ * turbid_gpu.h -- C ABI of libturbid_gpu.so, the B200 (sm_100a) implementation
+ * of TURBID's flat-bottom Fourier-Chebyshev RK3 substep.
+ *
+ * Plain C types only: host pointers for state exchange, device pointers (as
+ * double* or float*) for the field-container primitives, an opaque context.
+ * Every entry point returns a tg_status (0 = success); tg_last_error() gives
+ * a message in the reference's "Class::Method > text" style.
+ *
+ * Each entry point names the reference interface it replaces (paths relative
+ * to the yueliangyi/TURBID source tree).
+ *
+ * Device layouts used by the primitives:
+ *   physical field   [dim][Nz][Ny][Nx]      real, x fastest (as the reference)
+ *   spectral field   [dim][Nz][M]           complex (re,im) pairs, m fastest,
+ *                                            m = iy + Nyc*ix ("z-slab" layout)
+ *   host state (tg_upload_state / tg_download_state) uses the reference's
+ *   restart layout ccube(Nz, Nyc, Nxh*dim): [dim][Nxh][Nyc][Nz], z fastest.
+ *
+ * Threading: one host thread per context; all work is ordered on the
+ * context's CUDA stream; entry points are not reentrant on one context.
+ */
+#ifndef TURBID_GPU_H_
+#define TURBID_GPU_H_
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define TG_API __attribute__((visibility("default")))
+#else
+#define TG_API
+#endif
+
+typedef int tg_status;
+#define TG_OK            0
+#define TG_ERR_CUDA      1   /* a CUDA runtime call or kernel launch failed      */
+#define TG_ERR_SHAPE     2   /* unsupported or inconsistent grid / buffer sizes  */
+#define TG_ERR_ARG       3   /* invalid argument (null pointer, bad stage, ...)  */
+#define TG_ERR_NAN       4   /* non-finite value detected in the features        */
+#define TG_ERR_SETUP     5   /* operator construction failed (eigen-solver)      */
+#define TG_ERR_NOMEM     6   /* device allocation failed                         */
+#define TG_ERR_STATE     7   /* call out of order (e.g. step before upload)      */
+#define TG_ERR_TIMEOUT   8   /* a bounded device wait gave up                    */
+
+#define TG_PREC_FP64   0     /* all arithmetic in FP64 (parity mode)             */
+#define TG_PREC_MIXED  1     /* transforms and nonlinear products in FP32,
+                                z-operators and Helmholtz solves in FP64         */
+
+#define TG_NFEATURE 50       /* Phase::featureglobal_ (src/phase.cc:16-17)       */
+
+/* One case = the .ini parameters the hot path reads
+ * (src/configure.h:51-118; read by the Configuration::Load methods). */
+typedef struct tg_case {
+  int    nx, ny, nz;                 /* [Domain] grid_point_number              */
+  double lx, ly;                     /* [Domain] dimensionless_length (lz == 2) */
+  int    nphase;                     /* [System] total_phase_number (1 or 2)    */
+  int    mapping;                    /* [Space Stepper] 0 None,1 TwoEndTangent,
+                                        2 TwoEndSin, 3 OneEndTangent            */
+  double mapping_coef;
+  double slope; int slope_direction; /* [Domain] top_bottom_slope, direction    */
+  double dt;                         /* [Time Stepper] marching_time_step       */
+  int    output_based_on_step;
+  double reynolds, froude, averaged_concentration, specific_gravity;
+  int    affected_by_scalar;
+  double bc_u[5], bc_v[5], bc_w[5], bc_p[5];  /* vertical_type_u1/u2/u3/p      */
+  int    force_type;                 /* 0 None 1 Constant 2 Oscillatory
+                                        3 Pulsatile 4 Damping                   */
+  int    force_direction[2];
+  double force_amplitude[4];
+  double schmidt, settling, erosion_rate, critical_shear;
+  int    scalar_bc;                  /* 0 ZeroFlux, 1 ErosionDeposition         */
+  int    precision;                  /* TG_PREC_FP64 or TG_PREC_MIXED           */
+} tg_case;
+
+typedef struct tg_ctx tg_ctx;
+
+TG_API const char* tg_last_error(void);
+TG_API int tg_version(void);
+/* Number of kernels this library has launched so far in the process
+ * (no reference counterpart; measurement support). */
+TG_API long long tg_launch_count(void);
+
+/* Replaces System::System + DomainDecomposition::Configure (src/system.cc:19-64,
+ * src/base.cc:202-342), Domain::Configure (src/domain.cc:292-347),
+ * ChebyshevSpaceStepper::Configure (src/stepper_space_chebyshev.cc:101-250) and
+ * the decompositions built in FlatCarrierPhase::Configure /
+ * FlatScalarPhase::Configure (src/phase_carrier_flat.cc:178-246,
+ * src/phase_scalar_flat.cc:176-221, src/cmdz2_decomposition.cc:19-227).
+ * Operators are built on the host (own eigen-solver); allocates device memory. */
+TG_API tg_status tg_create(const tg_case* c, tg_ctx** out);
+TG_API tg_status tg_destroy(tg_ctx* ctx);
+/* dims = {nx, ny, nz, nxh, nyc, M} */
+TG_API tg_status tg_get_dims(const tg_ctx* ctx, int dims[6]);
+/* Use a caller's CUDA stream (cudaStream_t passed as void*); NULL = own stream. */
+TG_API tg_status tg_set_stream(tg_ctx* ctx, void* stream);
+TG_API tg_status tg_synchronize(tg_ctx* ctx);
+
+/* Replaces the matrices of CmDz2DecompositionCplx::Construct
+ * (src/cmdz2_decomposition.cc:19-227) with caller-supplied ones.
+ * which: 0 u, 1 v, 2 w, 3 p, 4 scalar.  Each matrix is nz*nz row-major FP64;
+ * E/Einv are the full matrices with the identity corners; lam has nz entries
+ * (rows 0 and nz-1 ignored); fbb/ftb/fbf/ftf are the four fix rows. */
+TG_API tg_status tg_set_decomposition(tg_ctx* ctx, int which, const double* E,
+                               const double* Einv, const double* lam,
+                               const double* fbb, const double* ftb,
+                               const double* fbf, const double* ftf);
+/* Reads back the operators built by tg_create (same layouts). */
+TG_API tg_status tg_get_decomposition(const tg_ctx* ctx, int which, double* E,
+                               double* Einv, double* lam, double* fbb,
+                               double* ftb, double* fbf, double* ftf);
+/* Host-only (no GPU needed): the operators tg_create builds, for a grid of
+ * nz Chebyshev points.  tg_operators_host replaces ChebyshevSpaceStepper::
+ * Configure (src/stepper_space_chebyshev.cc:101-250); tg_decomposition_host
+ * replaces CmDz2DecompositionCplx::Construct (src/cmdz2_decomposition.cc:19-227)
+ * for bc = {a_bottom, b_bottom, a_top, b_top}; outputs as in
+ * tg_get_decomposition. */
+TG_API tg_status tg_operators_host(int nz, int mapping, double mapping_coef, double* D1, double* D2);
+TG_API tg_status tg_decomposition_host(int nz, int mapping, double mapping_coef, const double* bc,
+                                double* E, double* Einv, double* lam, double* fbb,
+                                double* ftb, double* fbf, double* ftf);
+/* D1, D2 (nz*nz row-major) of ChebyshevSpaceStepper::Configure. */
+TG_API tg_status tg_get_operators(const tg_ctx* ctx, double* D1, double* D2);
+
+/* Replaces FlatCarrierVariable::Load / FlatScalarVariable::Load and the
+ * remainder of Variable::Configure (src/variable_carrier_flat.cc:262-421,
+ * src/variable_scalar_flat.cc). Host arrays in the restart layout: uvw is
+ * 3*Nxh*Nyc*Nz complex, p and phi Nxh*Nyc*Nz complex (phi may be NULL when
+ * nphase == 1).  Resets the RK3 registers and boundary history like a fresh
+ * Configure; sets step/time from start_step. */
+TG_API tg_status tg_upload_state(tg_ctx* ctx, const double* uvw, const double* p,
+                          const double* phi, int start_step);
+/* Replaces FlatCarrierVariable::Save / FlatScalarVariable::Save
+ * (src/variable_carrier_flat.cc:143-246): device -> host, same layout. */
+TG_API tg_status tg_download_state(tg_ctx* ctx, double* uvw, double* p, double* phi);
+
+/* Time bookkeeping of TimeStepper (src/stepper_time.h:56-91): the phases read
+ * time, dt, step and the alternation flag from here. */
+TG_API tg_status tg_set_time(tg_ctx* ctx, int step, double time, double dt, int alternation);
+TG_API tg_status tg_get_time(const tg_ctx* ctx, int* step, double* time, double* dt,
+                      int* alternation, int* isforward, double* cfl);
+
+/* Phase plugin methods (src/phase.h:25-114). */
+TG_API tg_status tg_carrier_predict(tg_ctx* ctx, int stage);  /* phase_carrier_flat.cc:272-559 */
+TG_API tg_status tg_carrier_correct(tg_ctx* ctx, int stage);  /* phase_carrier_flat.cc:566-709 */
+TG_API tg_status tg_scalar_predict(tg_ctx* ctx, int stage);   /* phase_scalar_flat.cc:245-284  */
+TG_API tg_status tg_scalar_correct(tg_ctx* ctx, int stage);   /* phase_scalar_flat.cc:291-533  */
+
+/* nsteps passes of the FlatChannelSolver::Execute loop body
+ * (src/solver_channel_flat.cc:199-293): TimeStepper::Update with the previous
+ * CFL feature, three stages of both phases, alternation flip.  Stops early when
+ * the CFL guard of TimeStepper::Update (src/stepper_time.cc:72-113) clears
+ * isForward.  maxstep / maxcfl as in [Time Stepper]; *done receives the number
+ * of steps taken (may be NULL).  When features is non-NULL it receives the
+ * 50-entry feature vector after the last step (one 400-byte device->host read). */
+TG_API tg_status tg_run_steps(tg_ctx* ctx, int nsteps, int maxstep, double maxcfl,
+                       double* features, int* done);
+
+/* Phase::GetFeatureGlobal (src/phase.h:57): 50 doubles, device -> host. */
+TG_API tg_status tg_features(tg_ctx* ctx, double* out);
+
+/* Kernel-class timing (no reference counterpart; measurement support):
+ * tg_profile_begin starts recording CUDA events around every instrumented
+ * launch on the context's stream; tg_profile_end synchronizes and returns per
+ * class the summed device milliseconds, algorithmic bytes and flops and the
+ * launch count.  Classes: 0 z-operator GEMM, 1 forward x pass, 2 forward y
+ * pass, 3 backward y pass, 4 backward x pass, 5 elementwise, 6 positivity
+ * filter, 7 feature reduction. */
+#define TG_PROF_NCAT 8
+TG_API tg_status tg_profile_begin(tg_ctx* ctx);
+TG_API tg_status tg_profile_end(tg_ctx* ctx, int ncat, double* ms, double* bytes,
+                                double* flops, int* count);
+
+/* Field-container primitives on device buffers (layouts above). */
+/* RealCplxCube::DftForward (src/cube_real_cplx.cc:525-539): pruned x r2c,
+ * y c2c, scaled 1/(NxNy).  phys: dim physical fields; spec: dim spectral. */
+TG_API tg_status tg_dft_forward_f64(tg_ctx* ctx, const double* phys, double* spec, int dim);
+TG_API tg_status tg_dft_forward_f32(tg_ctx* ctx, const float* phys, double* spec, int dim);
+/* RealCplxCube::DftBackward (src/cube_real_cplx.cc:542-555): zero-fill, unscaled. */
+TG_API tg_status tg_dft_backward_f64(tg_ctx* ctx, const double* spec, double* phys, int dim);
+TG_API tg_status tg_dft_backward_f32(tg_ctx* ctx, const double* spec, float* phys, int dim);
+/* RealCplxCube::Multiply(cmat, RealCplxCube&) (src/cube_real_cplx.cc:461-471):
+ * out = A * in along z for dim components; A is nz*nz row-major FP64 host
+ * memory (copied to the device on each call). */
+TG_API tg_status tg_multiply(tg_ctx* ctx, const double* A_host, const double* in,
+                      double* out, int dim);
+/* CmDz2 solve of FlatCarrierPhase::Helmholtz / FlatScalarPhase::Helmholtz
+ * (src/phase_carrier_flat.cc:861-994, src/phase_scalar_flat.cc:635-667) for
+ * one spectral component: which as in tg_set_decomposition, stage 0..2;
+ * rhs is not modified (the reference modifies its target in place). */
+TG_API tg_status tg_helmholtz(tg_ctx* ctx, int which, int stage, const double* rhs,
+                       double* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TURBID_GPU_H_ */

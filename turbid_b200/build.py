@@ -1,0 +1,66 @@
+"""Build recipe for libturbid_gpu.so (nvcc, sm_100a) -- built in-tree.
+
+    python -m turbid_b200.build        # or turbid_b200.build.build()
+
+The library is written next to this file so that it travels with the
+repository snapshot; nothing is installed into site-packages.
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+LIB = os.path.join(HERE, "libturbid_gpu.so")
+BUILD_DIR = os.path.join(HERE, "_build")
+
+CU_SOURCES = ["api.cu", "fft.cu", "gemm.cu", "fields.cu"]
+CC_SOURCES = ["setup.cc"]
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def _nvcc() -> str:
+    for cand in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", shutil.which("nvcc")):
+        if cand and os.path.exists(cand):
+            return cand
+    raise RuntimeError("nvcc not found")
+
+
+def _newer(target: str, sources) -> bool:
+    if not os.path.exists(target):
+        return False
+    t = os.path.getmtime(target)
+    return all(os.path.getmtime(s) <= t for s in sources)
+
+
+def build(verbose: bool = False, force: bool = False) -> str:
+    """Compile every CUDA/C++ source of the product into libturbid_gpu.so."""
+    srcs = [os.path.join(CSRC, s) for s in CU_SOURCES + CC_SOURCES]
+    headers = [os.path.join(CSRC, h) for h in os.listdir(CSRC) if h.endswith((".h", ".cuh"))]
+    headers.append(os.path.join(HERE, "..", "include", "turbid_gpu.h"))
+    if not force and _newer(LIB, srcs + headers):
+        return LIB
+    os.makedirs(BUILD_DIR, exist_ok=True)
+    nvcc = _nvcc()
+    objs = []
+    common = ["-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
+              "-lineinfo", "--expt-relaxed-constexpr"]
+    for s in srcs:
+        o = os.path.join(BUILD_DIR, os.path.basename(s) + ".o")
+        cmd = [nvcc, "-c", s, "-o", o] + ARCH + common
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.run(cmd, check=True)
+        objs.append(o)
+    cmd = [nvcc, "-shared", "-o", LIB] + objs + ARCH + ["-Xcompiler", "-fPIC"]
+    if verbose:
+        print(" ".join(cmd))
+    subprocess.run(cmd, check=True)
+    return LIB
+
+
+if __name__ == "__main__":
+    print(build(verbose=True, force="--force" in sys.argv))

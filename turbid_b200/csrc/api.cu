@@ -1,0 +1,1155 @@
+// C ABI of libturbid_gpu.so and the orchestration of the RK3 substep.
+//
+// One context = one case on one GPU.  The phase methods below follow the
+// reference's FlatCarrierPhase / FlatScalarPhase call sequence
+// (src/phase_carrier_flat.cc:272-709, src/phase_scalar_flat.cc:245-533) but
+// keep every field resident in HBM in the z-slab spectral layout, fold the
+// boundary fix rows into the two Helmholtz matrices, fuse the elementwise
+// Armadillo expressions into GEMM epilogues, and skip the transforms whose
+// results the reference never reads (only the bottom plane of du/dz, dv/dz
+// feeds the erosion flux; the scalar phase's physical velocity is the
+// carrier's plus a constant settling shift).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+
+#include "fields.cuh"
+#include "setup.h"
+#include "tg_common.cuh"
+
+namespace tg {
+
+thread_local std::string g_err;
+long long g_launches = 0;
+void set_error(const std::string& m) { g_err = m; }
+
+// columns: stage; rows: c1, c2, c3 (src/stepper_time_rk3.cc:28-31)
+static const double RK3[3][3] = {{0.0 / 1.0, -5.0 / 9.0, -153.0 / 128.0},
+                                 {1.0 / 3.0, 15.0 / 16.0, 8.0 / 15.0},
+                                 {1.0 / 6.0, 5.0 / 24.0, 1.0 / 8.0}};
+static const double kSmall = 10e-12;   // COMPARE_NUMBER_SMALL, src/common.h:42
+
+void fft_init();
+
+// ---------------------------------------------------------------------------
+// profiler: CUDA events around every instrumented launch, grouped by class
+// ---------------------------------------------------------------------------
+struct Profiler {
+  struct Rec {
+    int cat;
+    double bytes, flops;
+    cudaEvent_t a, b;
+  };
+  std::vector<Rec> recs;
+  std::vector<cudaEvent_t> pool;
+  size_t used = 0;
+  cudaEvent_t get() {
+    if (used < pool.size()) return pool[used++];
+    cudaEvent_t e;
+    TG_CUDA(cudaEventCreate(&e));
+    pool.push_back(e);
+    ++used;
+    return e;
+  }
+  void reset() {
+    recs.clear();
+    used = 0;
+  }
+  ~Profiler() {
+    for (auto e : pool) cudaEventDestroy(e);
+  }
+};
+thread_local Profiler* g_prof = nullptr;
+
+void prof_begin(cudaStream_t s, int cat, double bytes, double flops) {
+  if (!g_prof) return;
+  Profiler::Rec r{cat, bytes, flops, g_prof->get(), g_prof->get()};
+  TG_CUDA(cudaEventRecord(r.a, s));
+  g_prof->recs.push_back(r);
+}
+void prof_end(cudaStream_t s) {
+  if (!g_prof || g_prof->recs.empty()) return;
+  TG_CUDA(cudaEventRecord(g_prof->recs.back().b, s));
+}
+
+struct Ctx {
+  tg_case c{};
+  int nx = 0, ny = 0, nz = 0, nxc = 0, nyc = 0, nxh = 0, M = 0;
+  size_t S = 0, P = 0;
+  bool mixed = false, scalar = false, opentop = false;
+  cudaStream_t s = nullptr;
+  bool own_stream = false;
+  std::vector<double> gridz, gridzc, gridlenz, D1h, D2h;
+  double lmx = 0, lmy = 0;
+  Decomposition dec[5];
+  // device constants
+  double *kx = nullptr, *ky = nullptr, *dx2 = nullptr, *dy2 = nullptr, *k2 = nullptr;
+  double *gz = nullptr, *glz = nullptr, *d1r0 = nullptr, *d1rn = nullptr;
+  int* yidx = nullptr;
+  double *D1p = nullptr, *D2p = nullptr, *Atmp = nullptr;
+  int lda = 0, rowsPad = 0;
+  double* Einvf[5] = {nullptr};
+  double* Ef[5] = {nullptr};
+  double* lamd[5] = {nullptr};
+  FftPlan px, py;
+  TransformDims td{};
+  // device fields
+  double2 *U = nullptr, *PR = nullptr, *H = nullptr, *DP = nullptr, *SU = nullptr, *RHS = nullptr, *TMP = nullptr;
+  double2 *ADV = nullptr, *DU = nullptr, *F6 = nullptr, *PHI = nullptr, *HPHI = nullptr, *ADVPHI = nullptr;
+  double2 *RHSPHI = nullptr, *hist = nullptr, *ero = nullptr, *REF = nullptr;
+  void *UNL = nullptr, *DUP = nullptr, *PRD = nullptr, *PHIP = nullptr, *PLN = nullptr, *work = nullptr;
+  double* feat = nullptr;
+  unsigned long long* bits = nullptr;
+  double* feat_h = nullptr;   // pinned [2][100]
+  cudaEvent_t fev[2] = {nullptr, nullptr};
+  std::vector<void*> allocs;
+  Profiler prof;
+  // time / phase state
+  int step = 0;
+  double time = 0, dt = 0, olddt = 0, cfl = 0;
+  bool alternation = false, isforward = true, loaded = false;
+  double sig_u[3] = {0, 0, 0}, sig_s[3] = {0, 0, 0};
+  double shift[3] = {0, 0, 0};
+
+  template <typename X>
+  X* dalloc(size_t n) {
+    void* p = nullptr;
+    if (n == 0) n = 1;
+    cudaError_t e = cudaMalloc(&p, n * sizeof(X));
+    if (e != cudaSuccess) throw Error{TG_ERR_NOMEM, std::string("tg_create > cudaMalloc > ") + cudaGetErrorString(e)};
+    allocs.push_back(p);
+    TG_CUDA(cudaMemset(p, 0, n * sizeof(X)));
+    return reinterpret_cast<X*>(p);
+  }
+  ~Ctx() {
+    for (void* p : allocs) cudaFree(p);
+    if (feat_h) cudaFreeHost(feat_h);
+    for (auto& e : fev)
+      if (e) cudaEventDestroy(e);
+    fft_plan_destroy(px);
+    fft_plan_destroy(py);
+    if (own_stream && s) cudaStreamDestroy(s);
+  }
+  size_t psize() const { return mixed ? sizeof(float) : sizeof(double); }
+};
+
+// ---------------------------------------------------------------------------
+// construction
+// ---------------------------------------------------------------------------
+static void upload_padded(Ctx& x, double* dst, const std::vector<double>& A) {
+  std::vector<double> pad((size_t)x.rowsPad * x.lda, 0.0);
+  for (int i = 0; i < x.nz; ++i)
+    for (int j = 0; j < x.nz; ++j) pad[(size_t)i * x.lda + j] = A[(size_t)i * x.nz + j];
+  TG_CUDA(cudaMemcpy(dst, pad.data(), pad.size() * sizeof(double), cudaMemcpyHostToDevice));
+}
+
+static void install_decomposition(Ctx& x, int which) {
+  std::vector<double> Ei, E;
+  fold_decomposition(x.dec[which], which == 3, Ei, E);
+  upload_padded(x, x.Einvf[which], Ei);
+  upload_padded(x, x.Ef[which], E);
+  TG_CUDA(cudaMemcpy(x.lamd[which], x.dec[which].lam.data(), sizeof(double) * x.nz, cudaMemcpyHostToDevice));
+}
+
+static Ctx* create(const tg_case& c) {
+  if (c.nx < 1 || c.ny < 1 || c.nz < 3) throw Error{TG_ERR_SHAPE, "DomainDecomposition::Configure > Empty Data Dimension is not Supported!"};
+  if (c.nphase < 1 || c.nphase > 2) throw Error{TG_ERR_ARG, "tg_create > total_phase_number must be 1 or 2"};
+  if (c.precision != TG_PREC_FP64 && c.precision != TG_PREC_MIXED) throw Error{TG_ERR_ARG, "tg_create > unknown precision"};
+  std::unique_ptr<Ctx> px(new Ctx);
+  Ctx& x = *px;
+  x.c = c;
+  x.nx = c.nx;
+  x.ny = c.ny;
+  x.nz = c.nz;
+  x.nxc = c.nx / 3 * 2;   // src/base.cc:233-234
+  x.nyc = c.ny / 3 * 2;
+  x.nxh = x.nxc / 2 + 1;
+  x.M = x.nyc * x.nxh;
+  if (x.nyc < 1) throw Error{TG_ERR_SHAPE, "DomainDecomposition::Configure > Ny too small for the 2/3 cut"};
+  x.S = (size_t)x.nz * x.M;
+  x.P = (size_t)x.nx * x.ny * x.nz;
+  x.mixed = c.precision == TG_PREC_MIXED;
+  x.scalar = c.nphase > 1;
+  x.opentop = std::fabs(c.bc_u[2] - 0) <= kSmall && std::fabs(c.bc_u[3] - 1) <= kSmall;  // boundary.cc:59-71
+  x.dt = c.dt;
+  x.olddt = c.dt;
+  TG_CUDA(cudaStreamCreateWithFlags(&x.s, cudaStreamNonBlocking));
+  x.own_stream = true;
+  zgemm_init();
+  fft_init();
+
+  // grids (src/domain.cc:304-332) and operators (stepper_space_chebyshev.cc)
+  chebyshev_operators(x.nz, c.mapping, c.mapping_coef, x.gridz, x.D1h, x.D2h, x.gridzc);
+  {
+    std::vector<double> gx(x.nx), gy(x.ny);
+    for (int i = 0; i < x.nx; ++i) gx[i] = c.lx / x.nx * i;
+    for (int i = 0; i < x.ny; ++i) gy[i] = c.ly / x.ny * i;
+    x.lmx = c.lx;
+    for (int i = 0; i + 1 < x.nx; ++i) x.lmx = std::min(x.lmx, gx[i + 1] - gx[i]);
+    x.lmy = c.ly;
+    for (int i = 0; i + 1 < x.ny; ++i) x.lmy = std::min(x.lmy, gy[i + 1] - gy[i]);
+    const std::vector<double>& g = x.gridzc;
+    x.gridlenz.assign(x.nz, 0.0);
+    for (int k = 0; k < x.nz; ++k) {
+      if (k == 0)
+        x.gridlenz[k] = (g[1] - g[0]) / 2;
+      else if (k == x.nz - 1)
+        x.gridlenz[k] = (g[x.nz - 1] - g[x.nz - 2]) / 2;
+      else
+        x.gridlenz[k] = std::min(g[k + 1] - g[k], g[k] - g[k - 1]);
+    }
+  }
+  // wavenumbers per column m = iy + nyc*ix (src/stepper_space.cc:196-213)
+  {
+    const double pi = 3.141592653589793238462643383279502884;
+    const double kx1 = 2 * pi / c.lx, ky1 = 2 * pi / c.ly;
+    std::vector<double> kx(x.M), ky(x.M), dx2(x.M), dy2(x.M), k2(x.M);
+    for (int ix = 0; ix < x.nxh; ++ix)
+      for (int iy = 0; iy < x.nyc; ++iy) {
+        const int m = iy + x.nyc * ix;
+        double kxn = kx1 * (ix - 0);
+        double kym = (iy <= x.nyc / 2) ? +ky1 * (iy - 0) : -ky1 * (x.nyc - iy);
+        kx[m] = kxn;
+        ky[m] = kym;
+        dx2[m] = -std::pow(kxn, 2);
+        dy2[m] = -std::pow(kym, 2);
+        k2[m] = dx2[m] + dy2[m];
+      }
+    std::vector<int> yidx(x.nyc);
+    const int h = x.nyc / 2;
+    for (int iy = 0; iy < x.nyc; ++iy) yidx[iy] = iy < h ? iy : x.ny - (x.nyc - iy);
+    x.kx = x.dalloc<double>(x.M);
+    x.ky = x.dalloc<double>(x.M);
+    x.dx2 = x.dalloc<double>(x.M);
+    x.dy2 = x.dalloc<double>(x.M);
+    x.k2 = x.dalloc<double>(x.M);
+    x.yidx = x.dalloc<int>(x.nyc);
+    TG_CUDA(cudaMemcpy(x.kx, kx.data(), sizeof(double) * x.M, cudaMemcpyHostToDevice));
+    TG_CUDA(cudaMemcpy(x.ky, ky.data(), sizeof(double) * x.M, cudaMemcpyHostToDevice));
+    TG_CUDA(cudaMemcpy(x.dx2, dx2.data(), sizeof(double) * x.M, cudaMemcpyHostToDevice));
+    TG_CUDA(cudaMemcpy(x.dy2, dy2.data(), sizeof(double) * x.M, cudaMemcpyHostToDevice));
+    TG_CUDA(cudaMemcpy(x.k2, k2.data(), sizeof(double) * x.M, cudaMemcpyHostToDevice));
+    TG_CUDA(cudaMemcpy(x.yidx, yidx.data(), sizeof(int) * x.nyc, cudaMemcpyHostToDevice));
+  }
+  x.gz = x.dalloc<double>(x.nz);
+  x.glz = x.dalloc<double>(x.nz);
+  x.d1r0 = x.dalloc<double>(x.nz);
+  x.d1rn = x.dalloc<double>(x.nz);
+  TG_CUDA(cudaMemcpy(x.gz, x.gridz.data(), sizeof(double) * x.nz, cudaMemcpyHostToDevice));
+  TG_CUDA(cudaMemcpy(x.glz, x.gridlenz.data(), sizeof(double) * x.nz, cudaMemcpyHostToDevice));
+  TG_CUDA(cudaMemcpy(x.d1r0, x.D1h.data(), sizeof(double) * x.nz, cudaMemcpyHostToDevice));
+  TG_CUDA(cudaMemcpy(x.d1rn, x.D1h.data() + (size_t)(x.nz - 1) * x.nz, sizeof(double) * x.nz,
+                     cudaMemcpyHostToDevice));
+
+  // operators (padded for the GEMM tiles)
+  x.lda = (x.nz + 15) / 16 * 16;
+  x.rowsPad = (x.nz + 63) / 64 * 64;
+  const size_t opsz = (size_t)x.rowsPad * x.lda;
+  x.D1p = x.dalloc<double>(opsz);
+  x.D2p = x.dalloc<double>(opsz);
+  x.Atmp = x.dalloc<double>(opsz);
+  upload_padded(x, x.D1p, x.D1h);
+  upload_padded(x, x.D2p, x.D2h);
+  // decompositions: u, v, w, p (phase_carrier_flat.cc:186-201), scalar (phase_scalar_flat.cc:186-200)
+  const double* bcs[4] = {c.bc_u, c.bc_v, c.bc_w, c.bc_p};
+  for (int s = 0; s < 3; ++s) x.sig_u[s] = -c.reynolds / c.dt / RK3[2][s];
+  const int ndec = x.scalar ? 5 : 4;
+  for (int w = 0; w < ndec; ++w) {
+    double bc[4];
+    if (w < 4) {
+      for (int k = 0; k < 4; ++k) bc[k] = bcs[w][k];
+    } else {
+      const double rsw = c.reynolds * c.schmidt * c.settling;
+      bc[0] = rsw * 10e6;   // BOUNDARY_COEF_SCALE, src/common.h:55
+      bc[1] = 1 * 10e6;
+      bc[2] = rsw * 10e6;
+      bc[3] = 1 * 10e6;
+      for (int s = 0; s < 3; ++s) x.sig_s[s] = -c.reynolds * c.schmidt / c.dt / RK3[2][s];
+    }
+    try {
+      build_decomposition(x.nz, x.D1h, x.D2h, bc, x.dec[w]);
+    } catch (std::exception& e) {
+      throw Error{TG_ERR_SETUP, std::string("CmDz2DecompositionCplx::Construct > ") + e.what()};
+    }
+    x.Einvf[w] = x.dalloc<double>(opsz);
+    x.Ef[w] = x.dalloc<double>(opsz);
+    x.lamd[w] = x.dalloc<double>(x.nz);
+    install_decomposition(x, w);
+  }
+
+  // transforms
+  fft_plan_create(x.px, x.nx);
+  fft_plan_create(x.py, x.ny);
+  x.td.nx = x.nx;
+  x.td.ny = x.ny;
+  x.td.nz = x.nz;
+  x.td.nxh = x.nxh;
+  x.td.nyc = x.nyc;
+  x.td.M = x.M;
+  x.td.yidx = x.yidx;
+
+  // fields
+  const size_t S = x.S, P = x.P;
+  x.U = x.dalloc<double2>(3 * S);
+  x.PR = x.dalloc<double2>(S);
+  x.H = x.dalloc<double2>(3 * S);
+  x.DP = x.dalloc<double2>(3 * S);
+  x.SU = x.dalloc<double2>(3 * S);
+  x.RHS = x.dalloc<double2>(3 * S);
+  x.TMP = x.dalloc<double2>(3 * S);
+  x.ADV = x.dalloc<double2>(3 * S);
+  x.DU = x.dalloc<double2>(9 * S);
+  x.F6 = x.dalloc<double2>(6 * S);
+  x.REF = x.dalloc<double2>(3 * S);
+  x.hist = x.dalloc<double2>(24 * (size_t)x.M);
+  if (x.scalar) {
+    x.PHI = x.dalloc<double2>(S);
+    x.HPHI = x.dalloc<double2>(S);
+    x.ADVPHI = x.dalloc<double2>(S);
+    x.RHSPHI = x.dalloc<double2>(S);
+    x.ero = x.dalloc<double2>(x.M);
+  }
+  const size_t ps = x.psize();
+  x.UNL = x.dalloc<unsigned char>(3 * P * ps);
+  x.DUP = x.dalloc<unsigned char>(9 * P * ps);
+  x.PRD = x.dalloc<unsigned char>(6 * P * ps);
+  x.PHIP = x.dalloc<unsigned char>(P * ps);
+  x.PLN = x.dalloc<unsigned char>(3 * (size_t)x.nx * x.ny * ps);
+  x.work = x.dalloc<double2>(9 * (size_t)x.nz * x.nxh * x.ny);
+  x.feat = x.dalloc<double>(100);
+  x.bits = x.dalloc<unsigned long long>(16);
+  TG_CUDA(cudaMallocHost(&x.feat_h, 2 * 100 * sizeof(double)));
+  std::memset(x.feat_h, 0, 2 * 100 * sizeof(double));
+  TG_CUDA(cudaEventCreateWithFlags(&x.fev[0], cudaEventDisableTiming));
+  TG_CUDA(cudaEventCreateWithFlags(&x.fev[1], cudaEventDisableTiming));
+  return px.release();
+}
+
+// ---------------------------------------------------------------------------
+// helpers
+// ---------------------------------------------------------------------------
+static void gemm(Ctx& x, const double* A, const double2* in, long long sin, double2* out, long long sout, int batch,
+                 EpiParams ep) {
+  ep.nz = x.nz;
+  ep.M = x.M;
+  zgemm(A, x.lda, x.nz, x.nz, in, sin, out, sout, x.M, batch, ep, x.s);
+}
+
+template <typename T>
+static void fwd(Ctx& x, const void* phys, double2* spec, int planes) {
+  for (int p0 = 0; p0 < planes; p0 += 9 * x.nz) {
+    int np = std::min(planes - p0, 9 * x.nz);
+    dft_forward<T>(x.td, x.px, x.py, (const T*)phys + (size_t)p0 * x.nx * x.ny, spec + (size_t)p0 * x.M, np,
+                   x.work, x.s);
+  }
+}
+template <typename T>
+static void bwd(Ctx& x, const double2* spec, void* phys, int planes) {
+  for (int p0 = 0; p0 < planes; p0 += 9 * x.nz) {
+    int np = std::min(planes - p0, 9 * x.nz);
+    dft_backward<T>(x.td, x.px, x.py, spec + (size_t)p0 * x.M, (T*)phys + (size_t)p0 * x.nx * x.ny, np, x.work,
+                    x.s);
+  }
+}
+
+// driving force of the mean mode (src/phase_carrier_flat.cc:365-501)
+static void mean_force(const Ctx& x, double& f1, double& f2) {
+  const tg_case& c = x.c;
+  const double dt = x.dt, t = x.time;
+  const double tt = c.output_based_on_step ? t - dt / 2 : t + dt / 2;
+  f1 = f2 = 0;
+  const int* fd = c.force_direction;
+  const double* fa = c.force_amplitude;
+  switch (c.force_type) {
+    case 0:
+      break;
+    case 1:
+      if (fd[0] == 1) f1 = fa[0];
+      if (fd[0] == 2) f2 = fa[0];
+      break;
+    case 2: {
+      double a = fa[1];
+      if (fd[1] == 1) f1 = a * std::cos(a * tt);
+      if (fd[1] == 2) f2 = a * std::cos(a * tt);
+    } break;
+    case 3: {
+      if (fd[0] == 1) f1 = fa[0];
+      if (fd[0] == 2) f2 = fa[0];
+      double a = fa[1];
+      if (fd[1] == 1) f1 = f1 + a * std::cos(a * tt);
+      if (fd[1] == 2) f2 = f2 + a * std::cos(a * tt);
+    } break;
+    case 4: {
+      if (fd[0] == 1) f1 = fa[0];
+      if (fd[0] == 2) f2 = fa[0];
+      double a = fa[1];
+      const double T = fa[0], t0 = fa[1], lastp = fa[2], tarp = fa[3];
+      const double damp = -std::log(tarp) / (lastp + 0.25) / T;
+      double v = (a * std::cos(a * tt) - damp * std::sin(a * tt)) * std::exp(-damp * (t - t0));
+      if (fd[1] == 1) f1 = f1 + v;
+      if (fd[1] == 2) f2 = f2 + v;
+    } break;
+    default:
+      throw Error{TG_ERR_ARG, "FlatCarrierPhase::Predict() > Not Supported Force Type!"};
+  }
+}
+
+// ---------------------------------------------------------------------------
+// FlatCarrierPhase::Predict
+// ---------------------------------------------------------------------------
+template <typename T>
+static void carrier_predict(Ctx& x, int stage) {
+  const double dt = x.dt, c1 = RK3[0][stage], c2 = RK3[1][stage], c3 = RK3[2][stage];
+  const size_t S = x.S, P = x.P;
+  T* unl = (T*)x.UNL;
+  T* prd = (T*)x.PRD;
+  T* dup = (T*)x.DUP;
+  auto grad_u = [&]() {  // SpaceStepper::Gradient(uvw, d*dxyz, i) for i = 0..2
+    EpiParams ep;
+    ep.mode = EPI_GRAD;
+    ep.kx = x.kx;
+    ep.ky = x.ky;
+    ep.X0 = x.U;
+    ep.sX = S;
+    ep.aux0 = x.DU;
+    ep.aux1 = x.DU + S;
+    ep.sAux = 3 * S;
+    gemm(x, x.D1p, x.U, S, x.DU + 2 * S, 3 * S, 3, ep);
+  };
+  // NonlinearVelocity (phase_carrier_flat.cc:716-813)
+  if (x.alternation) {
+    products6<T>(unl, prd, P, x.s);
+    fwd<T>(x, prd, x.F6, 6 * x.nz);
+    // adv_i = d/dx(u_i u) + d/dy(u_i v) + d/dz(u_i w): GradientTmp + sum
+    const int inI[3] = {2, 4, 5}, x0I[3] = {0, 1, 2}, x1I[3] = {1, 3, 4};
+    for (int i = 0; i < 3; ++i) {
+      EpiParams ep;
+      ep.mode = EPI_DIV;
+      ep.kx = x.kx;
+      ep.ky = x.ky;
+      ep.X0 = x.F6 + x0I[i] * S;
+      ep.X1 = x.F6 + x1I[i] * S;
+      ep.s = 1.0;
+      gemm(x, x.D1p, x.F6 + inI[i] * S, S, x.ADV + i * S, S, 1, ep);
+    }
+    grad_u();
+  } else {
+    grad_u();
+    bwd<T>(x, x.DU, dup, 9 * x.nz);
+    adv_products<T>(unl, dup, prd, P, 3, 0.0, 0.0, 0.0, x.s);
+    fwd<T>(x, prd, x.ADV, 3 * x.nz);
+  }
+  if (x.scalar && x.c.scalar_bc == 1) {
+    // bottom plane of du/dz, dv/dz in physical space for the erosion flux
+    const size_t pl = (size_t)x.nx * x.ny;
+    bwd<T>(x, x.DU + 2 * S, (T*)x.PLN, 1);
+    bwd<T>(x, x.DU + 5 * S, (T*)x.PLN + pl, 1);
+  }
+  // H = c1 H - dt adv; buoyancy; mean-mode force
+  double bcoef = 0.0;
+  const double2* phi = nullptr;
+  if (x.scalar && x.c.affected_by_scalar) {
+    bcoef = dt * x.c.averaged_concentration / std::pow(x.c.froude, 2) * (x.c.specific_gravity - 1);
+    phi = x.PHI;
+  }
+  double f1, f2;
+  mean_force(x, f1, f2);
+  h_update(x.H, x.ADV, phi, S, x.M, c1, dt, bcoef, std::sin(x.c.slope), std::cos(x.c.slope), x.c.slope_direction,
+           dt * f1, dt * f2, x.s);
+  // Laplacian and rhs (phase_carrier_flat.cc:517-536)
+  {
+    const double redtc3 = -x.c.reynolds / dt / c3;
+    EpiParams ep;
+    ep.mode = EPI_LAPRHS;
+    ep.H = x.H;
+    ep.sH = S;
+    ep.U = x.U;
+    ep.sU = S;
+    ep.dx2 = x.dx2;
+    ep.dy2 = x.dy2;
+    ep.a = redtc3;
+    ep.c2 = c2;
+    gemm(x, x.D2p, x.U, S, x.RHS, S, 3, ep);
+  }
+  // FlatCarrierBoundary::Apply (boundary_carrier_flat.cc:185-246) + top mean values
+  {
+    const double c3m0 = RK3[2][stage], c3m1 = RK3[2][(stage + 2) % 3], c3m2 = RK3[2][(stage + 1) % 3];
+    double xm0 = 0, xm1 = 0, xm2 = 0;
+    switch (stage) {
+      case 0:
+        xm0 = 2 * (0 + c3m0) * dt;
+        xm1 = 0;
+        xm2 = 2 * (0 - c3m1) * x.olddt;
+        break;
+      case 1:
+        xm0 = 2 * (c3m0 + c3m1 + 0) * dt;
+        xm1 = 2 * (0 + c3m1 + 0) * dt;
+        xm2 = 0;
+        break;
+      default:
+        xm0 = 2 * (c3m0 + c3m1 + c3m2) * dt;
+        xm1 = 2 * (0 + c3m1 + c3m2) * dt;
+        xm2 = 2 * (0 + +0 + c3m2) * dt;
+        break;
+    }
+    const double r = (xm0 - xm1) / (xm1 - xm2);
+    boundary_apply(x.RHS, x.hist, S, x.M, x.nz, 2 * dt * c3m0, r, x.opentop ? 1 : 0, x.c.bc_u[4], x.c.bc_v[4],
+                   x.c.bc_w[4], x.s);
+  }
+  // Helmholtz, predict branch (phase_carrier_flat.cc:861-931)
+  for (int i = 0; i < 3; ++i) {
+    EpiParams ep;
+    ep.mode = EPI_RSCALE;
+    ep.lam = x.lamd[i];
+    ep.k2 = x.k2;
+    ep.sigma = x.sig_u[stage];
+    ep.null_mode = std::fabs(ep.sigma) < kSmall;
+    gemm(x, x.Einvf[i], x.RHS + i * S, S, x.TMP + i * S, S, 1, ep);
+    gemm(x, x.Ef[i], x.TMP + i * S, S, x.SU + i * S, S, 1, EpiParams());
+  }
+}
+
+// ---------------------------------------------------------------------------
+// FlatCarrierPhase::Correct
+// ---------------------------------------------------------------------------
+template <typename T>
+static void carrier_correct(Ctx& x, int stage) {
+  const double dt = x.dt, c3 = RK3[2][stage];
+  const size_t S = x.S;
+  {  // divergence of u* and pressure rhs (phase_carrier_flat.cc:586-589)
+    EpiParams ep;
+    ep.mode = EPI_DIV;
+    ep.kx = x.kx;
+    ep.ky = x.ky;
+    ep.X0 = x.SU;
+    ep.X1 = x.SU + S;
+    ep.s = 0.5 / dt / c3;
+    gemm(x, x.D1p, x.SU + 2 * S, S, x.TMP, S, 1, ep);
+  }
+  {  // Helmholtz, correction branch (phase_carrier_flat.cc:933-987)
+    EpiParams ep;
+    ep.mode = EPI_RSCALE;
+    ep.lam = x.lamd[3];
+    ep.k2 = x.k2;
+    ep.sigma = 0.0;
+    ep.null_mode = 1;
+    gemm(x, x.Einvf[3], x.TMP, S, x.TMP + S, S, 1, ep);
+    gemm(x, x.Ef[3], x.TMP + S, S, x.PR, S, 1, EpiParams());
+  }
+  {  // grad p (phase_carrier_flat.cc:597)
+    EpiParams ep;
+    ep.mode = EPI_GRAD;
+    ep.kx = x.kx;
+    ep.ky = x.ky;
+    ep.X0 = x.PR;
+    ep.aux0 = x.DP;
+    ep.aux1 = x.DP + S;
+    gemm(x, x.D1p, x.PR, S, x.DP + 2 * S, S, 1, ep);
+  }
+  if (stage == 2) x.olddt = dt;   // boundary_carrier_flat.cc:140-142
+  boundary_update(x.hist, x.DP, S, x.M, x.nz, x.opentop ? 1 : 0, x.kx, x.ky, x.d1r0, x.d1rn, x.s);
+  project(x.U, x.SU, x.DP, S, x.M, 2 * dt * c3, x.s);
+  bwd<T>(x, x.U, x.UNL, 3 * x.nz);
+  if (stage == 2)
+    features<T>((const T*)x.UNL, x.nx, x.ny, x.nz, x.glz, x.lmx, x.lmy, x.bits, x.feat, x.DU, S, x.M, x.s);
+}
+
+// ---------------------------------------------------------------------------
+// FlatScalarPhase::Predict / Correct
+// ---------------------------------------------------------------------------
+static void scalar_predict(Ctx& x, int) {
+  // u_phi = u with the settling shift of the mean mode (phase_scalar_flat.cc:258-279);
+  // its physical field is the carrier's plus this constant.
+  const tg_case& c = x.c;
+  x.shift[0] = x.shift[1] = 0.0;
+  if (c.slope_direction == 1) x.shift[0] = c.settling * std::sin(c.slope);
+  if (c.slope_direction == 2) x.shift[1] = c.settling * std::sin(c.slope);
+  x.shift[2] = -(c.settling * std::cos(c.slope));
+}
+
+template <typename T>
+static void scalar_correct(Ctx& x, int stage) {
+  const tg_case& c = x.c;
+  const double dt = x.dt, c1 = RK3[0][stage], c2 = RK3[1][stage], c3 = RK3[2][stage];
+  const size_t S = x.S, P = x.P, pl = (size_t)x.nx * x.ny;
+  T* unl = (T*)x.UNL;
+  T* prd = (T*)x.PRD;
+  T* dup = (T*)x.DUP;
+  T* phip = (T*)x.PHIP;
+  T* pln = (T*)x.PLN;
+  const double s0 = x.shift[0], s1 = x.shift[1], s2 = x.shift[2];
+  // NonlinearPressure (phase_scalar_flat.cc:552-599)
+  if (x.alternation) {
+    bwd<T>(x, x.PHI, phip, x.nz);
+    phi_products<T>(phip, unl, prd, P, s0, s1, s2, x.s);
+    fwd<T>(x, prd, x.F6, 3 * x.nz);
+    EpiParams ep;
+    ep.mode = EPI_DIV;
+    ep.kx = x.kx;
+    ep.ky = x.ky;
+    ep.X0 = x.F6;
+    ep.X1 = x.F6 + S;
+    ep.s = 1.0;
+    gemm(x, x.D1p, x.F6 + 2 * S, S, x.ADVPHI, S, 1, ep);
+  } else {
+    EpiParams ep;
+    ep.mode = EPI_GRAD;
+    ep.kx = x.kx;
+    ep.ky = x.ky;
+    ep.X0 = x.PHI;
+    ep.aux0 = x.TMP;
+    ep.aux1 = x.TMP + S;
+    gemm(x, x.D1p, x.PHI, S, x.TMP + 2 * S, S, 1, ep);
+    bwd<T>(x, x.TMP, dup, 3 * x.nz);
+    adv_products<T>(unl, dup, prd, P, 1, s0, s1, s2, x.s);
+    fwd<T>(x, prd, x.ADVPHI, x.nz);
+  }
+  axmby(x.HPHI, x.ADVPHI, S, c1, dt, x.s);
+  {  // lap phi and rhs (phase_scalar_flat.cc:313-329)
+    const double redtc3 = -c.reynolds * c.schmidt / dt / c3;
+    EpiParams ep;
+    ep.mode = EPI_LAPRHS;
+    ep.H = x.HPHI;
+    ep.U = x.PHI;
+    ep.dx2 = x.dx2;
+    ep.dy2 = x.dy2;
+    ep.a = redtc3;
+    ep.c2 = c2;
+    gemm(x, x.D2p, x.PHI, S, x.RHSPHI, S, 1, ep);
+  }
+  zero_rows(x.RHSPHI, x.M, x.nz, x.s);   // FlatScalarBoundary::Apply
+  if (c.scalar_bc == 1) {                 // erosion / deposition row (phase_scalar_flat.cc:340-384)
+    erosion_tau<T>(pln, pln + pl, pln + 2 * pl, pl, c.reynolds, c.critical_shear, c.erosion_rate, x.s);
+    fwd<T>(x, pln + 2 * pl, x.ero, 1);
+    erosion_row(x.RHSPHI, x.ero, x.PHI, x.M, c.settling * std::cos(c.slope), c.averaged_concentration,
+                c.reynolds * c.schmidt, x.feat, x.s);
+  }
+  {  // Helmholtz (phase_scalar_flat.cc:635-667)
+    EpiParams ep;
+    ep.mode = EPI_RSCALE;
+    ep.lam = x.lamd[4];
+    ep.k2 = x.k2;
+    ep.sigma = x.sig_s[stage];
+    ep.null_mode = std::fabs(ep.sigma) < kSmall;
+    gemm(x, x.Einvf[4], x.RHSPHI, S, x.TMP, S, 1, ep);
+    gemm(x, x.Ef[4], x.TMP, S, x.PHI, S, 1, EpiParams());
+  }
+  // Bartnicki positivity filter (phase_scalar_flat.cc:419-478)
+  bwd<T>(x, x.PHI, phip, x.nz);
+  positivity_filter<T>(phip, (int)pl, x.nz, x.s);
+  fwd<T>(x, phip, x.PHI, x.nz);
+  trapz_mean(x.PHI, x.M, x.nz, x.gz, 0.0, x.feat, 21, x.s);
+  if (stage == 2 && c.slope_direction > 0) {
+    trapz_mean(x.U, x.M, x.nz, x.gz, s0, x.feat, 22, x.s);
+    trapz_mean(x.U + S, x.M, x.nz, x.gz, s1, x.feat, 24, x.s);
+    set_feat(x.feat, 23, 0.0, x.s);
+    set_feat(x.feat, 25, 0.0, x.s);
+    if (x.step % 10 == 0) {
+      mul_shift<T>(phip, unl, prd, P, s0, x.s);
+      fwd<T>(x, prd, x.TMP, x.nz);
+      trapz_mean(x.TMP, x.M, x.nz, x.gz, 0.0, x.feat, 23, x.s);
+      mul_shift<T>(phip, unl + P, prd, P, s1, x.s);
+      fwd<T>(x, prd, x.TMP, x.nz);
+      trapz_mean(x.TMP, x.M, x.nz, x.gz, 0.0, x.feat, 25, x.s);
+    }
+  }
+}
+
+template <typename T>
+static void run_stage(Ctx& x, int stage) {
+  carrier_predict<T>(x, stage);
+  carrier_correct<T>(x, stage);
+  if (x.scalar) {
+    scalar_predict(x, stage);
+    scalar_correct<T>(x, stage);
+  }
+}
+
+static void upload_state(Ctx& x, const double* uvw, const double* p, const double* phi, int start_step) {
+  const size_t S = x.S;
+  TG_CUDA(cudaMemcpyAsync(x.REF, uvw, 3 * S * sizeof(double2), cudaMemcpyHostToDevice, x.s));
+  ref_to_slab(x.REF, x.U, x.M, x.nz, 3, x.s);
+  TG_CUDA(cudaMemcpyAsync(x.REF, p, S * sizeof(double2), cudaMemcpyHostToDevice, x.s));
+  ref_to_slab(x.REF, x.PR, x.M, x.nz, 1, x.s);
+  if (x.scalar) {
+    if (!phi) throw Error{TG_ERR_ARG, "FlatScalarVariable::Load > phi is required when nphase == 2"};
+    TG_CUDA(cudaMemcpyAsync(x.REF, phi, S * sizeof(double2), cudaMemcpyHostToDevice, x.s));
+    ref_to_slab(x.REF, x.PHI, x.M, x.nz, 1, x.s);
+    TG_CUDA(cudaMemsetAsync(x.HPHI, 0, S * sizeof(double2), x.s));
+  }
+  // FlatCarrierVariable::Configure: grad p, physical velocity; fresh registers
+  EpiParams ep;
+  ep.mode = EPI_GRAD;
+  ep.kx = x.kx;
+  ep.ky = x.ky;
+  ep.X0 = x.PR;
+  ep.aux0 = x.DP;
+  ep.aux1 = x.DP + S;
+  gemm(x, x.D1p, x.PR, S, x.DP + 2 * S, S, 1, ep);
+  TG_CUDA(cudaMemsetAsync(x.H, 0, 3 * S * sizeof(double2), x.s));
+  TG_CUDA(cudaMemsetAsync(x.hist, 0, 24 * (size_t)x.M * sizeof(double2), x.s));
+  TG_CUDA(cudaMemsetAsync(x.DU, 0, 9 * S * sizeof(double2), x.s));
+  TG_CUDA(cudaMemsetAsync(x.feat, 0, 100 * sizeof(double), x.s));
+  if (x.mixed)
+    bwd<float>(x, x.U, x.UNL, 3 * x.nz);
+  else
+    bwd<double>(x, x.U, x.UNL, 3 * x.nz);
+  x.olddt = x.dt;
+  x.step = std::max(0, start_step);
+  x.time = x.step * x.dt;
+  x.isforward = true;
+  x.alternation = false;
+  x.cfl = 0.0;
+  std::memset(x.feat_h, 0, 2 * 100 * sizeof(double));
+  x.loaded = true;
+}
+
+static void download_state(Ctx& x, double* uvw, double* p, double* phi) {
+  const size_t S = x.S;
+  slab_to_ref(x.U, x.REF, x.M, x.nz, 3, x.s);
+  TG_CUDA(cudaMemcpyAsync(uvw, x.REF, 3 * S * sizeof(double2), cudaMemcpyDeviceToHost, x.s));
+  TG_CUDA(cudaStreamSynchronize(x.s));
+  slab_to_ref(x.PR, x.REF, x.M, x.nz, 1, x.s);
+  TG_CUDA(cudaMemcpyAsync(p, x.REF, S * sizeof(double2), cudaMemcpyDeviceToHost, x.s));
+  TG_CUDA(cudaStreamSynchronize(x.s));
+  if (x.scalar && phi) {
+    slab_to_ref(x.PHI, x.REF, x.M, x.nz, 1, x.s);
+    TG_CUDA(cudaMemcpyAsync(phi, x.REF, S * sizeof(double2), cudaMemcpyDeviceToHost, x.s));
+  }
+  TG_CUDA(cudaStreamSynchronize(x.s));
+}
+
+// FlatChannelSolver::Execute loop body; the CFL guard of TimeStepper::Update
+// for step n+1 uses the features of step n, read back while step n+1 runs.
+static int run_steps(Ctx& x, int nsteps, int maxstep, double maxcfl, double* feat_out) {
+  if (!x.loaded) throw Error{TG_ERR_STATE, "FlatChannelSolver::Execute > state not loaded"};
+  int done = 0;
+  int pending = -1;           // slot of the feature copy of the previous step
+  double prev_f19 = x.feat_h[50 + 19];
+  for (int k = 0; k < nsteps && x.isforward; ++k) {
+    // TimeStepper::Update (src/stepper_time.cc:72-113); the CFL uses the features of
+    // the previous step, which are only needed once this step is enqueued.
+    x.step += 1;
+    x.time = x.time + x.dt;
+    bool fwd_flag = x.step < maxstep;
+    if (x.mixed) {
+      for (int st = 0; st < 3; ++st) run_stage<float>(x, st);
+    } else {
+      for (int st = 0; st < 3; ++st) run_stage<double>(x, st);
+    }
+    x.alternation = !x.alternation;
+    const int slot = done & 1;
+    TG_CUDA(cudaMemcpyAsync(x.feat_h + slot * 100, x.feat, 100 * sizeof(double), cudaMemcpyDeviceToHost, x.s));
+    TG_CUDA(cudaEventRecord(x.fev[slot], x.s));
+    if (pending >= 0) {
+      TG_CUDA(cudaEventSynchronize(x.fev[pending]));
+      prev_f19 = x.feat_h[pending * 100 + 50 + 19];
+    }
+    x.cfl = prev_f19 * x.dt;
+    if (!std::isfinite(prev_f19)) throw Error{TG_ERR_NAN, "TimeStepper::Update > non-finite CFL feature"};
+    if (x.cfl > maxcfl) fwd_flag = false;
+    x.isforward = fwd_flag;
+    pending = slot;
+    ++done;
+  }
+  TG_CUDA(cudaStreamSynchronize(x.s));
+  if (pending >= 0) {
+    std::memcpy(x.feat_h + 100 * (pending ^ 1), x.feat_h + 100 * pending, 100 * sizeof(double));
+    if (feat_out) std::memcpy(feat_out, x.feat_h + pending * 100 + 50, 50 * sizeof(double));
+    if (!std::isfinite(x.feat_h[pending * 100 + 50 + 19]))
+      throw Error{TG_ERR_NAN, "FlatCarrierPhase::Correct > non-finite velocity features"};
+  }
+  return done;
+}
+
+}  // namespace tg
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+using namespace tg;
+
+#define TG_TRY(...)                                          \
+  try {                                                      \
+    __VA_ARGS__;                                             \
+    return TG_OK;                                            \
+  } catch (const Error& e) {                                 \
+    set_error(e.msg);                                        \
+    return e.code;                                           \
+  } catch (const std::exception& e) {                        \
+    set_error(e.what());                                     \
+    return TG_ERR_SETUP;                                     \
+  }
+
+#define TG_CHECK_CTX(x) \
+  if (!(x)) { set_error("null context"); return TG_ERR_ARG; }
+
+extern "C" {
+
+const char* tg_last_error(void) { return g_err.c_str(); }
+int tg_version(void) { return 1; }
+long long tg_launch_count(void) { return g_launches; }
+
+tg_status tg_create(const tg_case* c, tg_ctx** out) {
+  if (!c || !out) {
+    set_error("tg_create > null argument");
+    return TG_ERR_ARG;
+  }
+  TG_TRY(*out = reinterpret_cast<tg_ctx*>(create(*c)));
+}
+
+tg_status tg_destroy(tg_ctx* ctx) {
+  TG_CHECK_CTX(ctx);
+  TG_TRY(delete reinterpret_cast<Ctx*>(ctx));
+}
+
+tg_status tg_get_dims(const tg_ctx* ctx, int dims[6]) {
+  TG_CHECK_CTX(ctx);
+  const Ctx& x = *reinterpret_cast<const Ctx*>(ctx);
+  dims[0] = x.nx;
+  dims[1] = x.ny;
+  dims[2] = x.nz;
+  dims[3] = x.nxh;
+  dims[4] = x.nyc;
+  dims[5] = x.M;
+  return TG_OK;
+}
+
+tg_status tg_set_stream(tg_ctx* ctx, void* stream) {
+  TG_CHECK_CTX(ctx);
+  Ctx& x = *reinterpret_cast<Ctx*>(ctx);
+  TG_TRY({
+    TG_CUDA(cudaStreamSynchronize(x.s));
+    if (stream) {
+      if (x.own_stream) cudaStreamDestroy(x.s);
+      x.s = reinterpret_cast<cudaStream_t>(stream);
+      x.own_stream = false;
+    } else if (!x.own_stream) {
+      TG_CUDA(cudaStreamCreateWithFlags(&x.s, cudaStreamNonBlocking));
+      x.own_stream = true;
+    }
+  });
+}
+
+tg_status tg_synchronize(tg_ctx* ctx) {
+  TG_CHECK_CTX(ctx);
+  TG_TRY(TG_CUDA(cudaStreamSynchronize(reinterpret_cast<Ctx*>(ctx)->s)));
+}
+
+tg_status tg_set_decomposition(tg_ctx* ctx, int which, const double* E, const double* Einv, const double* lam,
+                               const double* fbb, const double* ftb, const double* fbf, const double* ftf) {
+  TG_CHECK_CTX(ctx);
+  Ctx& x = *reinterpret_cast<Ctx*>(ctx);
+  if (which < 0 || which > 4 || (which == 4 && !x.scalar) || !E || !Einv || !lam || !fbb || !ftb || !fbf || !ftf) {
+    set_error("tg_set_decomposition > bad argument");
+    return TG_ERR_ARG;
+  }
+  TG_TRY({
+    const size_t nn = (size_t)x.nz * x.nz;
+    Decomposition& d = x.dec[which];
+    d.n = x.nz;
+    d.E.assign(E, E + nn);
+    d.Einv.assign(Einv, Einv + nn);
+    d.lam.assign(lam, lam + x.nz);
+    d.fbb.assign(fbb, fbb + x.nz);
+    d.ftb.assign(ftb, ftb + x.nz);
+    d.fbf.assign(fbf, fbf + x.nz);
+    d.ftf.assign(ftf, ftf + x.nz);
+    TG_CUDA(cudaStreamSynchronize(x.s));
+    install_decomposition(x, which);
+  });
+}
+
+tg_status tg_get_decomposition(const tg_ctx* ctx, int which, double* E, double* Einv, double* lam, double* fbb,
+                               double* ftb, double* fbf, double* ftf) {
+  TG_CHECK_CTX(ctx);
+  const Ctx& x = *reinterpret_cast<const Ctx*>(ctx);
+  if (which < 0 || which > 4 || (which == 4 && !x.scalar)) {
+    set_error("tg_get_decomposition > bad argument");
+    return TG_ERR_ARG;
+  }
+  const Decomposition& d = x.dec[which];
+  auto cp = [](double* dst, const std::vector<double>& v) {
+    if (dst) std::memcpy(dst, v.data(), v.size() * sizeof(double));
+  };
+  cp(E, d.E);
+  cp(Einv, d.Einv);
+  cp(lam, d.lam);
+  cp(fbb, d.fbb);
+  cp(ftb, d.ftb);
+  cp(fbf, d.fbf);
+  cp(ftf, d.ftf);
+  return TG_OK;
+}
+
+tg_status tg_get_operators(const tg_ctx* ctx, double* D1, double* D2) {
+  TG_CHECK_CTX(ctx);
+  const Ctx& x = *reinterpret_cast<const Ctx*>(ctx);
+  if (D1) std::memcpy(D1, x.D1h.data(), x.D1h.size() * sizeof(double));
+  if (D2) std::memcpy(D2, x.D2h.data(), x.D2h.size() * sizeof(double));
+  return TG_OK;
+}
+
+tg_status tg_operators_host(int nz, int mapping, double mapping_coef, double* D1, double* D2) {
+  if (nz < 3 || !D1 || !D2) {
+    set_error("tg_operators_host > bad argument");
+    return TG_ERR_ARG;
+  }
+  TG_TRY({
+    std::vector<double> gz, d1, d2, gzc;
+    chebyshev_operators(nz, mapping, mapping_coef, gz, d1, d2, gzc);
+    std::memcpy(D1, d1.data(), d1.size() * sizeof(double));
+    std::memcpy(D2, d2.data(), d2.size() * sizeof(double));
+  });
+}
+
+tg_status tg_decomposition_host(int nz, int mapping, double mapping_coef, const double* bc, double* E, double* Einv,
+                                double* lam, double* fbb, double* ftb, double* fbf, double* ftf) {
+  if (nz < 3 || !bc) {
+    set_error("tg_decomposition_host > bad argument");
+    return TG_ERR_ARG;
+  }
+  TG_TRY({
+    std::vector<double> gz, d1, d2, gzc;
+    chebyshev_operators(nz, mapping, mapping_coef, gz, d1, d2, gzc);
+    Decomposition d;
+    build_decomposition(nz, d1, d2, bc, d);
+    auto cp = [](double* dst, const std::vector<double>& v) {
+      if (dst) std::memcpy(dst, v.data(), v.size() * sizeof(double));
+    };
+    cp(E, d.E);
+    cp(Einv, d.Einv);
+    cp(lam, d.lam);
+    cp(fbb, d.fbb);
+    cp(ftb, d.ftb);
+    cp(fbf, d.fbf);
+    cp(ftf, d.ftf);
+  });
+}
+
+tg_status tg_upload_state(tg_ctx* ctx, const double* uvw, const double* p, const double* phi, int start_step) {
+  TG_CHECK_CTX(ctx);
+  if (!uvw || !p) {
+    set_error("FlatCarrierVariable::Load > null state pointer");
+    return TG_ERR_ARG;
+  }
+  TG_TRY(upload_state(*reinterpret_cast<Ctx*>(ctx), uvw, p, phi, start_step));
+}
+
+tg_status tg_download_state(tg_ctx* ctx, double* uvw, double* p, double* phi) {
+  TG_CHECK_CTX(ctx);
+  Ctx& x = *reinterpret_cast<Ctx*>(ctx);
+  if (!uvw || !p) {
+    set_error("FlatCarrierVariable::Save > null state pointer");
+    return TG_ERR_ARG;
+  }
+  if (!x.loaded) {
+    set_error("FlatCarrierVariable::Save > state not loaded");
+    return TG_ERR_STATE;
+  }
+  TG_TRY(download_state(x, uvw, p, phi));
+}
+
+tg_status tg_set_time(tg_ctx* ctx, int step, double time, double dt, int alternation) {
+  TG_CHECK_CTX(ctx);
+  Ctx& x = *reinterpret_cast<Ctx*>(ctx);
+  if (dt != x.dt) {
+    set_error("tg_set_time > dt differs from the assembled decompositions (adaptive dt is not supported)");
+    return TG_ERR_ARG;
+  }
+  x.step = step;
+  x.time = time;
+  x.alternation = alternation != 0;
+  return TG_OK;
+}
+
+tg_status tg_get_time(const tg_ctx* ctx, int* step, double* time, double* dt, int* alternation, int* isforward,
+                      double* cfl) {
+  TG_CHECK_CTX(ctx);
+  const Ctx& x = *reinterpret_cast<const Ctx*>(ctx);
+  if (step) *step = x.step;
+  if (time) *time = x.time;
+  if (dt) *dt = x.dt;
+  if (alternation) *alternation = x.alternation;
+  if (isforward) *isforward = x.isforward;
+  if (cfl) *cfl = x.cfl;
+  return TG_OK;
+}
+
+#define TG_STAGE_CALL(fn_f32, fn_f64)                                     \
+  TG_CHECK_CTX(ctx);                                                      \
+  Ctx& x = *reinterpret_cast<Ctx*>(ctx);                                  \
+  if (stage < 0 || stage > 2) {                                           \
+    set_error("Phase > stage must be 0, 1 or 2");                         \
+    return TG_ERR_ARG;                                                    \
+  }                                                                       \
+  if (!x.loaded) {                                                        \
+    set_error("Phase > state not loaded");                                \
+    return TG_ERR_STATE;                                                  \
+  }                                                                       \
+  TG_TRY(if (x.mixed) fn_f32; else fn_f64;)
+
+tg_status tg_carrier_predict(tg_ctx* ctx, int stage) {
+  TG_STAGE_CALL(carrier_predict<float>(x, stage), carrier_predict<double>(x, stage));
+}
+tg_status tg_carrier_correct(tg_ctx* ctx, int stage) {
+  TG_STAGE_CALL(carrier_correct<float>(x, stage), carrier_correct<double>(x, stage));
+}
+static bool has_scalar(tg_ctx* ctx) {
+  if (ctx && reinterpret_cast<Ctx*>(ctx)->scalar) return true;
+  set_error("FlatScalarPhase > case has no scalar phase");
+  return false;
+}
+tg_status tg_scalar_predict(tg_ctx* ctx, int stage) {
+  if (ctx && !has_scalar(ctx)) return TG_ERR_STATE;
+  TG_STAGE_CALL(scalar_predict(x, stage), scalar_predict(x, stage));
+}
+tg_status tg_scalar_correct(tg_ctx* ctx, int stage) {
+  if (ctx && !has_scalar(ctx)) return TG_ERR_STATE;
+  TG_STAGE_CALL(scalar_correct<float>(x, stage), scalar_correct<double>(x, stage));
+}
+
+tg_status tg_run_steps(tg_ctx* ctx, int nsteps, int maxstep, double maxcfl, double* features, int* done) {
+  TG_CHECK_CTX(ctx);
+  Ctx& x = *reinterpret_cast<Ctx*>(ctx);
+  int d = 0;
+  tg_status st;
+  try {
+    d = run_steps(x, nsteps, maxstep, maxcfl, features);
+    st = TG_OK;
+  } catch (const Error& e) {
+    set_error(e.msg);
+    st = e.code;
+  }
+  if (done) *done = d;
+  return st;
+}
+
+tg_status tg_profile_begin(tg_ctx* ctx) {
+  TG_CHECK_CTX(ctx);
+  Ctx& x = *reinterpret_cast<Ctx*>(ctx);
+  TG_TRY({
+    TG_CUDA(cudaStreamSynchronize(x.s));
+    x.prof.reset();
+    g_prof = &x.prof;
+  });
+}
+
+tg_status tg_profile_end(tg_ctx* ctx, int ncat, double* ms, double* bytes, double* flops, int* count) {
+  TG_CHECK_CTX(ctx);
+  Ctx& x = *reinterpret_cast<Ctx*>(ctx);
+  TG_TRY({
+    g_prof = nullptr;
+    TG_CUDA(cudaStreamSynchronize(x.s));
+    for (int c = 0; c < ncat; ++c) {
+      if (ms) ms[c] = 0;
+      if (bytes) bytes[c] = 0;
+      if (flops) flops[c] = 0;
+      if (count) count[c] = 0;
+    }
+    for (auto& r : x.prof.recs) {
+      if (r.cat < 0 || r.cat >= ncat) continue;
+      float t = 0.f;
+      TG_CUDA(cudaEventElapsedTime(&t, r.a, r.b));
+      if (ms) ms[r.cat] += t;
+      if (bytes) bytes[r.cat] += r.bytes;
+      if (flops) flops[r.cat] += r.flops;
+      if (count) count[r.cat] += 1;
+    }
+    x.prof.reset();
+  });
+}
+
+tg_status tg_features(tg_ctx* ctx, double* out) {
+  TG_CHECK_CTX(ctx);
+  if (!out) {
+    set_error("tg_features > null output");
+    return TG_ERR_ARG;
+  }
+  Ctx& x = *reinterpret_cast<Ctx*>(ctx);
+  TG_TRY({
+    TG_CUDA(cudaMemcpyAsync(x.feat_h, x.feat, 100 * sizeof(double), cudaMemcpyDeviceToHost, x.s));
+    TG_CUDA(cudaStreamSynchronize(x.s));
+    std::memcpy(out, x.feat_h + 50, 50 * sizeof(double));
+  });
+}
+
+tg_status tg_dft_forward_f64(tg_ctx* ctx, const double* phys, double* spec, int dim) {
+  TG_CHECK_CTX(ctx);
+  Ctx& x = *reinterpret_cast<Ctx*>(ctx);
+  if (!phys || !spec || dim < 1) {
+    set_error("RealCplxCube::DftForward > bad argument");
+    return TG_ERR_ARG;
+  }
+  TG_TRY(fwd<double>(x, phys, reinterpret_cast<double2*>(spec), dim * x.nz));
+}
+tg_status tg_dft_forward_f32(tg_ctx* ctx, const float* phys, double* spec, int dim) {
+  TG_CHECK_CTX(ctx);
+  Ctx& x = *reinterpret_cast<Ctx*>(ctx);
+  if (!phys || !spec || dim < 1) {
+    set_error("RealCplxCube::DftForward > bad argument");
+    return TG_ERR_ARG;
+  }
+  TG_TRY(fwd<float>(x, phys, reinterpret_cast<double2*>(spec), dim * x.nz));
+}
+tg_status tg_dft_backward_f64(tg_ctx* ctx, const double* spec, double* phys, int dim) {
+  TG_CHECK_CTX(ctx);
+  Ctx& x = *reinterpret_cast<Ctx*>(ctx);
+  if (!phys || !spec || dim < 1) {
+    set_error("RealCplxCube::DftBackward > bad argument");
+    return TG_ERR_ARG;
+  }
+  TG_TRY(bwd<double>(x, reinterpret_cast<const double2*>(spec), phys, dim * x.nz));
+}
+tg_status tg_dft_backward_f32(tg_ctx* ctx, const double* spec, float* phys, int dim) {
+  TG_CHECK_CTX(ctx);
+  Ctx& x = *reinterpret_cast<Ctx*>(ctx);
+  if (!phys || !spec || dim < 1) {
+    set_error("RealCplxCube::DftBackward > bad argument");
+    return TG_ERR_ARG;
+  }
+  TG_TRY(bwd<float>(x, reinterpret_cast<const double2*>(spec), phys, dim * x.nz));
+}
+
+tg_status tg_multiply(tg_ctx* ctx, const double* A_host, const double* in, double* out, int dim) {
+  TG_CHECK_CTX(ctx);
+  Ctx& x = *reinterpret_cast<Ctx*>(ctx);
+  if (!A_host || !in || !out || dim < 1) {
+    set_error("RealCplxCube::Multiply > bad argument");
+    return TG_ERR_ARG;
+  }
+  if (in == out) {
+    set_error("RealCplxCube::Multiply(cmat,RealCplxCube) > Can not Do In-place Multiplication!");
+    return TG_ERR_ARG;
+  }
+  TG_TRY({
+    TG_CUDA(cudaStreamSynchronize(x.s));
+    std::vector<double> A(A_host, A_host + (size_t)x.nz * x.nz);
+    upload_padded(x, x.Atmp, A);
+    gemm(x, x.Atmp, reinterpret_cast<const double2*>(in), x.S, reinterpret_cast<double2*>(out), x.S, dim,
+         EpiParams());
+  });
+}
+
+tg_status tg_helmholtz(tg_ctx* ctx, int which, int stage, const double* rhs, double* out) {
+  TG_CHECK_CTX(ctx);
+  Ctx& x = *reinterpret_cast<Ctx*>(ctx);
+  if (which < 0 || which > 4 || (which == 4 && !x.scalar) || stage < 0 || stage > 2 || !rhs || !out) {
+    set_error("Phase::Helmholtz > bad argument");
+    return TG_ERR_ARG;
+  }
+  TG_TRY({
+    EpiParams ep;
+    ep.mode = EPI_RSCALE;
+    ep.lam = x.lamd[which];
+    ep.k2 = x.k2;
+    ep.sigma = which < 3 ? x.sig_u[stage] : (which == 3 ? 0.0 : x.sig_s[stage]);
+    ep.null_mode = std::fabs(ep.sigma) < kSmall;
+    gemm(x, x.Einvf[which], reinterpret_cast<const double2*>(rhs), x.S, x.TMP, x.S, 1, ep);
+    gemm(x, x.Ef[which], x.TMP, x.S, reinterpret_cast<double2*>(out), x.S, 1, EpiParams());
+  });
+}
+
+}  // extern "C"

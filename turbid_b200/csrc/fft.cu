@@ -1,0 +1,393 @@
+// Pruned plane transforms of RealCplxCube::DftForward / DftBackward
+// (reference src/cube_real_cplx.cc:525-555, pruning of P3DFFT's
+// build/ftran.F90:122-248 and build/btran.F90:137-243).
+//
+// Physical planes are x-fastest [plane][y][x]; spectral planes are the
+// z-slab layout [plane][m], m = iy + Nyc*ix.  A transform is two kernels:
+//   x pass: batched real FFT of two rows at a time packed as one complex FFT,
+//           only kx < Nxh kept, written column-major [plane][kx][y];
+//   y pass: complex FFT along y of each kept column, only the Nyc pruned
+//           wavenumbers kept (kx-major), scaled by 1/(Nx*Ny).
+// The 1-D FFTs are mixed-radix Stockham passes in shared memory with
+// twiddles from a table computed once per length on the host.
+#include <cmath>
+#include <cstring>
+
+#include "tg_common.cuh"
+
+namespace tg {
+
+// ---------------------------------------------------------------------------
+// plan: factorisation + twiddle table
+// ---------------------------------------------------------------------------
+void fft_plan_create(FftPlan& p, int L) {
+  p.L = L;
+  p.npass = 0;
+  int n = L;
+  auto push = [&](int r) {
+    if (p.npass >= kMaxPasses) throw Error{TG_ERR_SHAPE, "FftPlan > too many passes"};
+    p.rad[p.npass++] = r;
+  };
+  while (n % 4 == 0) { push(4); n /= 4; }
+  while (n % 2 == 0) { push(2); n /= 2; }
+  const int primes[] = {3, 5, 7, 11, 13};
+  for (int q : primes)
+    while (n % q == 0) { push(q); n /= q; }
+  if (n > 1) push(n);  // one direct DFT pass for the remaining factor
+  std::vector<double2> t64(L);
+  std::vector<float2> t32(L);
+  for (int k = 0; k < L; ++k) {
+    // angle -2 pi k / L evaluated in long double
+    long double a = -2.0L * 3.141592653589793238462643383279502884L * (long double)k / (long double)L;
+    long double c = cosl(a), s = sinl(a);
+    t64[k] = make_double2((double)c, (double)s);
+    t32[k] = make_float2((float)c, (float)s);
+  }
+  TG_CUDA(cudaMalloc(&p.tw64, sizeof(double2) * L));
+  TG_CUDA(cudaMalloc(&p.tw32, sizeof(float2) * L));
+  TG_CUDA(cudaMemcpy(p.tw64, t64.data(), sizeof(double2) * L, cudaMemcpyHostToDevice));
+  TG_CUDA(cudaMemcpy(p.tw32, t32.data(), sizeof(float2) * L, cudaMemcpyHostToDevice));
+}
+
+void fft_plan_destroy(FftPlan& p) {
+  if (p.tw64) cudaFree(p.tw64);
+  if (p.tw32) cudaFree(p.tw32);
+  p.tw64 = nullptr;
+  p.tw32 = nullptr;
+}
+
+struct PlanArgs {
+  int L, npass;
+  int rad[kMaxPasses];
+};
+
+static PlanArgs plan_args(const FftPlan& p) {
+  PlanArgs a;
+  a.L = p.L;
+  a.npass = p.npass;
+  for (int i = 0; i < kMaxPasses; ++i) a.rad[i] = p.rad[i];
+  return a;
+}
+
+// ---------------------------------------------------------------------------
+// device FFT of NB transforms of length L held in shared memory
+// DIR = -1: exp(-i...) (forward), DIR = +1: exp(+i...) (backward, unscaled)
+// ---------------------------------------------------------------------------
+template <typename T, int DIR>
+__device__ __forceinline__ cplx<T> tw_get(const cplx<T>* tw, int idx) {
+  cplx<T> w = tw[idx];
+  if (DIR > 0) w.y = -w.y;
+  return w;
+}
+
+template <typename T, int DIR>
+__device__ cplx<T>* fft_batch(cplx<T>* b0, cplx<T>* b1, int NB, const PlanArgs& pl,
+                              const cplx<T>* __restrict__ tw) {
+  using C = cplx<T>;
+  const int L = pl.L;
+  C* in = b0;
+  C* out = b1;
+  int Ns = 1;
+  for (int ps = 0; ps < pl.npass; ++ps) {
+    const int R = pl.rad[ps];
+    const int nb = L / R;
+    const int twstep = L / (Ns * R);
+    for (int idx = threadIdx.x; idx < NB * nb; idx += blockDim.x) {
+      const int b = idx / nb;
+      const int j = idx - b * nb;
+      const C* src = in + b * L;
+      C* dst = out + b * L;
+      const int jm = j % Ns;
+      const int base = (j - jm) * R + jm;
+      if (R == 2) {
+        C a0 = src[j];
+        C a1 = cmul(src[j + nb], tw_get<T, DIR>(tw, jm * twstep));
+        dst[base] = cadd(a0, a1);
+        dst[base + Ns] = csub(a0, a1);
+      } else if (R == 4) {
+        C a0 = src[j];
+        C a1 = cmul(src[j + nb], tw_get<T, DIR>(tw, jm * twstep));
+        C a2 = cmul(src[j + 2 * nb], tw_get<T, DIR>(tw, 2 * jm * twstep));
+        C a3 = cmul(src[j + 3 * nb], tw_get<T, DIR>(tw, 3 * jm * twstep));
+        C t0 = cadd(a0, a2), t1 = csub(a0, a2), t2 = cadd(a1, a3), t3 = csub(a1, a3);
+        // DIR=-1: multiply t3 by -i ; DIR=+1: by +i
+        C t3r = (DIR < 0) ? mkc<C>(t3.y, -t3.x) : mkc<C>(-t3.y, t3.x);
+        dst[base] = cadd(t0, t2);
+        dst[base + Ns] = cadd(t1, t3r);
+        dst[base + 2 * Ns] = csub(t0, t2);
+        dst[base + 3 * Ns] = csub(t1, t3r);
+      } else if (R <= 16) {
+        C v[16];
+        for (int r = 0; r < R; ++r) v[r] = cmul(src[j + r * nb], tw_get<T, DIR>(tw, jm * r * twstep));
+        const int ws = L / R;
+        for (int k = 0; k < R; ++k) {
+          C acc = v[0];
+          for (int r = 1; r < R; ++r) acc = cadd(acc, cmul(v[r], tw_get<T, DIR>(tw, ((r * k) % R) * ws)));
+          dst[base + k * Ns] = acc;
+        }
+      } else {
+        const int ws = L / R;
+        for (int k = 0; k < R; ++k) {
+          C acc = mkc<C>(0, 0);
+          for (int r = 0; r < R; ++r) {
+            C x = cmul(src[j + r * nb], tw_get<T, DIR>(tw, jm * r * twstep));
+            acc = cadd(acc, cmul(x, tw_get<T, DIR>(tw, (int)(((long long)r * k) % R) * ws)));
+          }
+          dst[base + k * Ns] = acc;
+        }
+      }
+    }
+    __syncthreads();
+    C* t = in;
+    in = out;
+    out = t;
+    Ns *= R;
+  }
+  return in;
+}
+
+template <typename T> struct Tw;
+template <> struct Tw<double> {
+  static __host__ const double2* get(const FftPlan& p) { return p.tw64; }
+};
+template <> struct Tw<float> {
+  static __host__ const float2* get(const FftPlan& p) { return p.tw32; }
+};
+
+// ---------------------------------------------------------------------------
+// forward x pass: phys [plane][y][x] (T) -> work [plane][kx][y] (cplx<T>)
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(256) fwd_x_kernel(TransformDims d, PlanArgs pl, const cplx<T>* __restrict__ tw,
+                                                    const T* __restrict__ phys, cplx<T>* __restrict__ work, int NB) {
+  using C = cplx<T>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* b0 = reinterpret_cast<C*>(smem_raw);
+  C* b1 = b0 + NB * pl.L;
+  const int L = pl.L;  // == nx
+  const int plane = blockIdx.y;
+  const int y0 = blockIdx.x * 2 * NB;
+  const T* src = phys + (size_t)plane * d.ny * d.nx;
+  for (int idx = threadIdx.x; idx < NB * L; idx += blockDim.x) {
+    const int p = idx / L, x = idx - p * L;
+    const int ya = y0 + 2 * p, yb = ya + 1;
+    T re = ya < d.ny ? src[(size_t)ya * d.nx + x] : T(0);
+    T im = yb < d.ny ? src[(size_t)yb * d.nx + x] : T(0);
+    b0[idx] = mkc<C>(re, im);
+  }
+  __syncthreads();
+  C* r = fft_batch<T, -1>(b0, b1, NB, pl, tw);
+  const int rows = 2 * NB;
+  C* dst = work + (size_t)plane * d.nxh * d.ny;
+  for (int idx = threadIdx.x; idx < rows * d.nxh; idx += blockDim.x) {
+    const int k = idx / rows, q = idx - k * rows;
+    const int y = y0 + q;
+    if (y >= d.ny) continue;
+    const int p = q >> 1;
+    C Z = r[p * L + k];
+    C Zc = cconj(r[p * L + (k == 0 ? 0 : L - k)]);
+    C X;
+    if ((q & 1) == 0) {
+      X = mkc<C>((Z.x + Zc.x) * T(0.5), (Z.y + Zc.y) * T(0.5));
+    } else {
+      C D = csub(Z, Zc);
+      X = mkc<C>(D.y * T(0.5), -D.x * T(0.5));
+    }
+    dst[(size_t)k * d.ny + y] = X;
+  }
+}
+
+// forward y pass: work [plane][kx][y] -> spec [plane][iy + nyc*kx] (double2)
+template <typename T>
+__global__ void __launch_bounds__(256) fwd_y_kernel(TransformDims d, PlanArgs pl, const cplx<T>* __restrict__ tw,
+                                                    const cplx<T>* __restrict__ work, double2* __restrict__ spec,
+                                                    int NB, double scale) {
+  using C = cplx<T>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* b0 = reinterpret_cast<C*>(smem_raw);
+  C* b1 = b0 + NB * pl.L;
+  const int L = pl.L;  // == ny
+  const int plane = blockIdx.y;
+  const int k0 = blockIdx.x * NB;
+  const C* src = work + (size_t)plane * d.nxh * d.ny;
+  for (int idx = threadIdx.x; idx < NB * L; idx += blockDim.x) {
+    const int c = idx / L, y = idx - c * L;
+    const int k = k0 + c;
+    b0[idx] = k < d.nxh ? src[(size_t)k * d.ny + y] : mkc<C>(0, 0);
+  }
+  __syncthreads();
+  C* r = fft_batch<T, -1>(b0, b1, NB, pl, tw);
+  double2* dst = spec + (size_t)plane * d.M;
+  for (int idx = threadIdx.x; idx < NB * d.nyc; idx += blockDim.x) {
+    const int c = idx / d.nyc, iy = idx - c * d.nyc;
+    const int k = k0 + c;
+    if (k >= d.nxh) continue;
+    C v = r[c * L + d.yidx[iy]];
+    dst[iy + (size_t)d.nyc * k] = make_double2((double)v.x * scale, (double)v.y * scale);
+  }
+}
+
+// backward y pass: spec -> work (zero-filled pruned modes, unscaled)
+template <typename T>
+__global__ void __launch_bounds__(256) bwd_y_kernel(TransformDims d, PlanArgs pl, const cplx<T>* __restrict__ tw,
+                                                    const double2* __restrict__ spec, cplx<T>* __restrict__ work,
+                                                    int NB) {
+  using C = cplx<T>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* b0 = reinterpret_cast<C*>(smem_raw);
+  C* b1 = b0 + NB * pl.L;
+  const int L = pl.L;  // == ny
+  const int plane = blockIdx.y;
+  const int k0 = blockIdx.x * NB;
+  for (int idx = threadIdx.x; idx < NB * L; idx += blockDim.x) b0[idx] = mkc<C>(0, 0);
+  __syncthreads();
+  const double2* src = spec + (size_t)plane * d.M;
+  for (int idx = threadIdx.x; idx < NB * d.nyc; idx += blockDim.x) {
+    const int c = idx / d.nyc, iy = idx - c * d.nyc;
+    const int k = k0 + c;
+    if (k >= d.nxh) continue;
+    double2 v = src[iy + (size_t)d.nyc * k];
+    b0[c * L + d.yidx[iy]] = mkc<C>((T)v.x, (T)v.y);
+  }
+  __syncthreads();
+  C* r = fft_batch<T, +1>(b0, b1, NB, pl, tw);
+  C* dst = work + (size_t)plane * d.nxh * d.ny;
+  for (int idx = threadIdx.x; idx < NB * L; idx += blockDim.x) {
+    const int c = idx / L, y = idx - c * L;
+    const int k = k0 + c;
+    if (k < d.nxh) dst[(size_t)k * d.ny + y] = r[idx];
+  }
+}
+
+// backward x pass: work [plane][kx][y] -> phys [plane][y][x]; two rows per
+// complex FFT; the imaginary part of the kx = 0 coefficient is ignored (c2r).
+template <typename T>
+__global__ void __launch_bounds__(256) bwd_x_kernel(TransformDims d, PlanArgs pl, const cplx<T>* __restrict__ tw,
+                                                    const cplx<T>* __restrict__ work, T* __restrict__ phys, int NB) {
+  using C = cplx<T>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* b0 = reinterpret_cast<C*>(smem_raw);
+  C* b1 = b0 + NB * pl.L;
+  const int L = pl.L;  // == nx
+  const int plane = blockIdx.y;
+  const int y0 = blockIdx.x * 2 * NB;
+  for (int idx = threadIdx.x; idx < NB * L; idx += blockDim.x) b0[idx] = mkc<C>(0, 0);
+  __syncthreads();
+  const C* src = work + (size_t)plane * d.nxh * d.ny;
+  for (int idx = threadIdx.x; idx < NB * d.nxh; idx += blockDim.x) {
+    const int k = idx / NB, p = idx - k * NB;
+    const int ya = y0 + 2 * p, yb = ya + 1;
+    C h1 = ya < d.ny ? src[(size_t)k * d.ny + ya] : mkc<C>(0, 0);
+    C h2 = yb < d.ny ? src[(size_t)k * d.ny + yb] : mkc<C>(0, 0);
+    if (k == 0) {
+      h1.y = T(0);
+      h2.y = T(0);
+    }
+    // Z = X1 + i X2 with X[k] = h, X[L-k] = conj(h)
+    b0[p * L + k] = mkc<C>(h1.x - h2.y, h1.y + h2.x);
+    if (k > 0) b0[p * L + (L - k)] = mkc<C>(h1.x + h2.y, -h1.y + h2.x);
+  }
+  __syncthreads();
+  C* r = fft_batch<T, +1>(b0, b1, NB, pl, tw);
+  T* dst = phys + (size_t)plane * d.ny * d.nx;
+  for (int idx = threadIdx.x; idx < NB * L; idx += blockDim.x) {
+    const int p = idx / L, x = idx - p * L;
+    const int ya = y0 + 2 * p, yb = ya + 1;
+    C z = r[idx];
+    if (ya < d.ny) dst[(size_t)ya * d.nx + x] = z.x;
+    if (yb < d.ny) dst[(size_t)yb * d.nx + x] = z.y;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------
+static const size_t kFftSmemBudget = 64 * 1024;
+
+static int pick_nb(int L, size_t csize) {
+  const size_t budget = kFftSmemBudget;
+  if (2 * (size_t)L * csize > budget)
+    throw Error{TG_ERR_SHAPE, "RealCplxCube::DftForward > transform length too large for one CTA"};
+  int nb = (int)(budget / (2 * (size_t)L * csize));
+  if (nb > 16) nb = 16;
+  if (nb < 1) nb = 1;
+  return nb;
+}
+
+template <typename Kern>
+static void set_smem(Kern k) {
+  TG_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFftSmemBudget));
+}
+
+void fft_init() {
+  set_smem(fwd_x_kernel<double>);
+  set_smem(fwd_y_kernel<double>);
+  set_smem(bwd_y_kernel<double>);
+  set_smem(bwd_x_kernel<double>);
+  set_smem(fwd_x_kernel<float>);
+  set_smem(fwd_y_kernel<float>);
+  set_smem(bwd_y_kernel<float>);
+  set_smem(bwd_x_kernel<float>);
+}
+
+template <typename T>
+void dft_forward(const TransformDims& d, const FftPlan& px, const FftPlan& py, const T* phys, double2* spec,
+                 int planes, void* work, cudaStream_t s) {
+  using C = cplx<T>;
+  C* w = reinterpret_cast<C*>(work);
+  {
+    int nb = pick_nb(px.L, sizeof(C));
+    size_t sm = 2 * (size_t)nb * px.L * sizeof(C);
+    dim3 grid((d.ny + 2 * nb - 1) / (2 * nb), planes);
+    prof_begin(s, PC_FFT_FX, (double)planes * d.ny * (d.nx * sizeof(T) + d.nxh * sizeof(C)), 0);
+    fwd_x_kernel<T><<<grid, 256, sm, s>>>(d, plan_args(px), Tw<T>::get(px), phys, w, nb);
+    prof_end(s);
+    TG_LAUNCH_CHECK("fwd_x_kernel");
+  }
+  {
+    int nb = pick_nb(py.L, sizeof(C));
+    size_t sm = 2 * (size_t)nb * py.L * sizeof(C);
+    dim3 grid((d.nxh + nb - 1) / nb, planes);
+    prof_begin(s, PC_FFT_FY, (double)planes * ((double)d.nxh * d.ny * sizeof(C) + (double)d.M * sizeof(double2)), 0);
+    fwd_y_kernel<T><<<grid, 256, sm, s>>>(d, plan_args(py), Tw<T>::get(py), w, spec, nb,
+                                          1.0 / ((double)d.nx * (double)d.ny));
+    prof_end(s);
+    TG_LAUNCH_CHECK("fwd_y_kernel");
+  }
+}
+
+template <typename T>
+void dft_backward(const TransformDims& d, const FftPlan& px, const FftPlan& py, const double2* spec, T* phys,
+                  int planes, void* work, cudaStream_t s) {
+  using C = cplx<T>;
+  C* w = reinterpret_cast<C*>(work);
+  {
+    int nb = pick_nb(py.L, sizeof(C));
+    size_t sm = 2 * (size_t)nb * py.L * sizeof(C);
+    dim3 grid((d.nxh + nb - 1) / nb, planes);
+    prof_begin(s, PC_FFT_BY, (double)planes * ((double)d.nxh * d.ny * sizeof(C) + (double)d.M * sizeof(double2)), 0);
+    bwd_y_kernel<T><<<grid, 256, sm, s>>>(d, plan_args(py), Tw<T>::get(py), spec, w, nb);
+    prof_end(s);
+    TG_LAUNCH_CHECK("bwd_y_kernel");
+  }
+  {
+    int nb = pick_nb(px.L, sizeof(C));
+    size_t sm = 2 * (size_t)nb * px.L * sizeof(C);
+    dim3 grid((d.ny + 2 * nb - 1) / (2 * nb), planes);
+    prof_begin(s, PC_FFT_BX, (double)planes * d.ny * (d.nx * sizeof(T) + d.nxh * sizeof(C)), 0);
+    bwd_x_kernel<T><<<grid, 256, sm, s>>>(d, plan_args(px), Tw<T>::get(px), w, phys, nb);
+    prof_end(s);
+    TG_LAUNCH_CHECK("bwd_x_kernel");
+  }
+}
+
+template void dft_forward<double>(const TransformDims&, const FftPlan&, const FftPlan&, const double*, double2*, int,
+                                  void*, cudaStream_t);
+template void dft_forward<float>(const TransformDims&, const FftPlan&, const FftPlan&, const float*, double2*, int,
+                                 void*, cudaStream_t);
+template void dft_backward<double>(const TransformDims&, const FftPlan&, const FftPlan&, const double2*, double*, int,
+                                   void*, cudaStream_t);
+template void dft_backward<float>(const TransformDims&, const FftPlan&, const FftPlan&, const double2*, float*, int,
+                                  void*, cudaStream_t);
+
+}  // namespace tg

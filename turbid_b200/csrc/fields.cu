@@ -1,0 +1,499 @@
+// Elementwise stage kernels and reductions of the RK3 substep.
+// Each kernel restates one block of the reference's Armadillo expressions
+// (file:line cited per kernel), evaluated per element in the same order.
+#include "fields.cuh"
+
+namespace tg {
+
+namespace {
+constexpr int kT = 256;
+inline unsigned nblk(size_t n, int per = 1) {
+  size_t b = (n + (size_t)kT * per - 1) / ((size_t)kT * per);
+  if (b > 148u * 32u) b = 148u * 32u;   // grid-stride beyond ~32 CTAs per SM
+  return (unsigned)(b ? b : 1);
+}
+
+__device__ __forceinline__ double2 mul_i(double k, double2 x) {  // (0, k) * x
+  return make_double2(0.0 * x.x - k * x.y, 0.0 * x.y + k * x.x);
+}
+}  // namespace
+
+// --- layout conversion: reference [c][m][z] <-> slab [c][z][m] ---------------
+__global__ void k_ref_to_slab(const double2* __restrict__ ref, double2* __restrict__ slab, int M, int nz) {
+  __shared__ double2 t[32][33];
+  const int c = blockIdx.z;
+  const double2* src = ref + (size_t)c * M * nz;
+  double2* dst = slab + (size_t)c * M * nz;
+  const int z0 = blockIdx.x * 32, m0 = blockIdx.y * 32;
+  for (int i = threadIdx.y; i < 32; i += 8) {
+    int m = m0 + i, z = z0 + threadIdx.x;
+    if (m < M && z < nz) t[i][threadIdx.x] = src[(size_t)m * nz + z];
+  }
+  __syncthreads();
+  for (int i = threadIdx.y; i < 32; i += 8) {
+    int z = z0 + i, m = m0 + threadIdx.x;
+    if (m < M && z < nz) dst[(size_t)z * M + m] = t[threadIdx.x][i];
+  }
+}
+__global__ void k_slab_to_ref(const double2* __restrict__ slab, double2* __restrict__ ref, int M, int nz) {
+  __shared__ double2 t[32][33];
+  const int c = blockIdx.z;
+  const double2* src = slab + (size_t)c * M * nz;
+  double2* dst = ref + (size_t)c * M * nz;
+  const int z0 = blockIdx.x * 32, m0 = blockIdx.y * 32;
+  for (int i = threadIdx.y; i < 32; i += 8) {
+    int z = z0 + i, m = m0 + threadIdx.x;
+    if (m < M && z < nz) t[i][threadIdx.x] = src[(size_t)z * M + m];
+  }
+  __syncthreads();
+  for (int i = threadIdx.y; i < 32; i += 8) {
+    int m = m0 + i, z = z0 + threadIdx.x;
+    if (m < M && z < nz) dst[(size_t)m * nz + z] = t[threadIdx.x][i];
+  }
+}
+void ref_to_slab(const double2* ref, double2* slab, int M, int nz, int dim, cudaStream_t s) {
+  dim3 g((nz + 31) / 32, (M + 31) / 32, dim), b(32, 8);
+  k_ref_to_slab<<<g, b, 0, s>>>(ref, slab, M, nz);
+  TG_LAUNCH_CHECK("k_ref_to_slab");
+}
+void slab_to_ref(const double2* slab, double2* ref, int M, int nz, int dim, cudaStream_t s) {
+  dim3 g((nz + 31) / 32, (M + 31) / 32, dim), b(32, 8);
+  k_slab_to_ref<<<g, b, 0, s>>>(slab, ref, M, nz);
+  TG_LAUNCH_CHECK("k_slab_to_ref");
+}
+
+// --- physical products ---------------------------------------------------------
+// divergence form products u_i u_j (phase_carrier_flat.cc:725-745): the six
+// distinct ones uu, uv, uw, vv, vw, ww (u_i u_j == u_j u_i exactly).
+template <typename T>
+__global__ void k_products6(const T* __restrict__ unl, T* __restrict__ prd, size_t P) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < P; i += (size_t)gridDim.x * blockDim.x) {
+    T u = unl[i], v = unl[P + i], w = unl[2 * P + i];
+    prd[i] = u * u;
+    prd[P + i] = u * v;
+    prd[2 * P + i] = u * w;
+    prd[3 * P + i] = v * v;
+    prd[4 * P + i] = v * w;
+    prd[5 * P + i] = w * w;
+  }
+}
+template <typename T>
+void products6(const T* unl, T* prd, size_t P, cudaStream_t s) {
+  prof_begin(s, PC_ELEM, 9.0 * sizeof(T) * (double)P, 0);
+  k_products6<T><<<nblk(P), kT, 0, s>>>(unl, prd, P);
+  prof_end(s);
+  TG_LAUNCH_CHECK("k_products6");
+}
+
+// advective form out_i = u du_i/dx + v du_i/dy + w du_i/dz
+// (phase_carrier_flat.cc:786-797; phase_scalar_flat.cc:588-591 with dim = 1).
+// dup: ncomp x 3 physical gradient fields; sh: constant velocity shift (scalar
+// phase settling velocity, phase_scalar_flat.cc:258-279).
+template <typename T>
+__global__ void k_adv(const T* __restrict__ unl, const T* __restrict__ dup, T* __restrict__ out, size_t P, int ncomp,
+                      double su, double sv, double sw) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < P; i += (size_t)gridDim.x * blockDim.x) {
+    T u = unl[i] + (T)su, v = unl[P + i] + (T)sv, w = unl[2 * P + i] + (T)sw;
+    for (int c = 0; c < ncomp; ++c) {
+      const T* d = dup + (size_t)c * 3 * P;
+      out[(size_t)c * P + i] = u * d[i] + v * d[P + i] + w * d[2 * P + i];
+    }
+  }
+}
+template <typename T>
+void adv_products(const T* unl, const T* dup, T* out, size_t P, int ncomp, double su, double sv, double sw,
+                  cudaStream_t s) {
+  prof_begin(s, PC_ELEM, (3.0 + 4.0 * ncomp) * sizeof(T) * (double)P, 0);
+  k_adv<T><<<nblk(P), kT, 0, s>>>(unl, dup, out, P, ncomp, su, sv, sw);
+  prof_end(s);
+  TG_LAUNCH_CHECK("k_adv");
+}
+
+// phi * u_j (phase_scalar_flat.cc:563-569)
+template <typename T>
+__global__ void k_phi_products(const T* __restrict__ phip, const T* __restrict__ unl, T* __restrict__ out, size_t P,
+                               double su, double sv, double sw) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < P; i += (size_t)gridDim.x * blockDim.x) {
+    T p = phip[i];
+    out[i] = p * (unl[i] + (T)su);
+    out[P + i] = p * (unl[P + i] + (T)sv);
+    out[2 * P + i] = p * (unl[2 * P + i] + (T)sw);
+  }
+}
+template <typename T>
+void phi_products(const T* phip, const T* unl, T* out, size_t P, double su, double sv, double sw, cudaStream_t s) {
+  prof_begin(s, PC_ELEM, 7.0 * sizeof(T) * (double)P, 0);
+  k_phi_products<T><<<nblk(P), kT, 0, s>>>(phip, unl, out, P, su, sv, sw);
+  prof_end(s);
+  TG_LAUNCH_CHECK("k_phi_products");
+}
+
+// single product a * (b + shift) for the flux features (phase_scalar_flat.cc:500-518)
+template <typename T>
+__global__ void k_mul_shift(const T* __restrict__ a, const T* __restrict__ b, T* __restrict__ out, size_t P,
+                            double sh) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < P; i += (size_t)gridDim.x * blockDim.x)
+    out[i] = (b[i] + (T)sh) * a[i];
+}
+template <typename T>
+void mul_shift(const T* a, const T* b, T* out, size_t P, double sh, cudaStream_t s) {
+  prof_begin(s, PC_ELEM, 3.0 * sizeof(T) * (double)P, 0);
+  k_mul_shift<T><<<nblk(P), kT, 0, s>>>(a, b, out, P, sh);
+  prof_end(s);
+  TG_LAUNCH_CHECK("k_mul_shift");
+}
+
+// --- carrier H register (phase_carrier_flat.cc:293-296, 325-356, 503-504) -------
+__global__ void k_h_update(double2* __restrict__ H, const double2* __restrict__ adv, const double2* __restrict__ phi,
+                           size_t S, int M, double c1, double dt, double bcoef, double sinsl, double cossl, int sdir,
+                           double dtf1, double dtf2) {
+  const size_t n = 3 * S;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const int c = (int)(i / S);
+    const size_t e = i - (size_t)c * S;
+    const int m = (int)(e % M);
+    double2 h = H[i], a = adv[i];
+    h = make_double2(c1 * h.x - dt * a.x, c1 * h.y - dt * a.y);
+    if (phi) {
+      double2 p = phi[e];
+      if ((sdir == 1 && c == 0) || (sdir == 2 && c == 1)) {
+        h.x = h.x + bcoef * p.x * sinsl;
+        h.y = h.y + bcoef * p.y * sinsl;
+      }
+      if (c == 2) {
+        h.x = h.x - bcoef * p.x * cossl;
+        h.y = h.y - bcoef * p.y * cossl;
+      }
+    }
+    if (m == 0) {
+      if (c == 0) h.x += dtf1;
+      if (c == 1) h.x += dtf2;
+    }
+    H[i] = h;
+  }
+}
+void h_update(double2* H, const double2* adv, const double2* phi, size_t S, int M, double c1, double dt,
+              double bcoef, double sinsl, double cossl, int sdir, double dtf1, double dtf2, cudaStream_t s) {
+  prof_begin(s, PC_ELEM, 144.0 * (double)S, 0);
+  k_h_update<<<nblk(3 * S), kT, 0, s>>>(H, adv, phi, S, M, c1, dt, bcoef, sinsl, cossl, sdir, dtf1, dtf2);
+  prof_end(s);
+  TG_LAUNCH_CHECK("k_h_update");
+}
+
+// scalar register (phase_scalar_flat.cc:308-310)
+__global__ void k_axpby(double2* __restrict__ y, const double2* __restrict__ x, size_t n, double a, double b) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    double2 v = y[i], w = x[i];
+    y[i] = make_double2(a * v.x - b * w.x, a * v.y - b * w.y);
+  }
+}
+void axmby(double2* y, const double2* x, size_t n, double a, double b, cudaStream_t s) {
+  prof_begin(s, PC_ELEM, 48.0 * (double)n, 0);
+  k_axpby<<<nblk(n), kT, 0, s>>>(y, x, n, a, b);
+  prof_end(s);
+  TG_LAUNCH_CHECK("k_axpby");
+}
+
+// --- boundary rows ---------------------------------------------------------------
+// FlatCarrierBoundary::Apply (boundary_carrier_flat.cc:230-242) + the mean-mode
+// top values (phase_carrier_flat.cc:542-547).  hist: [8][3][M] rows
+// 0 dp1m1top 1 dp1m1bot 2 dp1m2top 3 dp1m2bot 4 dp2m1top 5 dp2m1bot 6 dp2m2top 7 dp2m2bot
+__global__ void k_boundary_apply(double2* __restrict__ rhs, const double2* __restrict__ hist, size_t S, int M, int nz,
+                                 double fac, double r, int opentop, double tu, double tv, double tw) {
+  const int n = 3 * M;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int c = i / M, m = i - c * M;
+    const double2* h = hist;
+    const size_t R = (size_t)3 * M;
+    double2 t1 = h[0 * R + i], t2 = h[2 * R + i], b1 = h[1 * R + i], b2 = h[3 * R + i];
+    double2 top = make_double2(fac * ((1 + r) * t1.x + (0 - r) * t2.x), fac * ((1 + r) * t1.y + (0 - r) * t2.y));
+    double2 bot = make_double2(fac * ((1 + r) * b1.x + (0 - r) * b2.x), fac * ((1 + r) * b1.y + (0 - r) * b2.y));
+    if (opentop && c < 2) {
+      double2 q1 = h[4 * R + i], q2 = h[6 * R + i];
+      top = make_double2(fac * ((1 + r) * q1.x + (0 - r) * q2.x), fac * ((1 + r) * q1.y + (0 - r) * q2.y));
+    }
+    if (m == 0) top = make_double2(c == 0 ? tu : (c == 1 ? tv : tw), 0.0);
+    rhs[(size_t)c * S + (size_t)(nz - 1) * M + m] = top;
+    rhs[(size_t)c * S + m] = bot;
+  }
+}
+void boundary_apply(double2* rhs, const double2* hist, size_t S, int M, int nz, double fac, double r, int opentop,
+                    double tu, double tv, double tw, cudaStream_t s) {
+  k_boundary_apply<<<nblk(3 * (size_t)M), kT, 0, s>>>(rhs, hist, S, M, nz, fac, r, opentop, tu, tv, tw);
+  TG_LAUNCH_CHECK("k_boundary_apply");
+}
+
+// FlatCarrierBoundary::Update (boundary_carrier_flat.cc:131-170): history
+// shift and new wall rows of grad p; with an open top the rows of grad(dp/dz)
+// (phase_carrier_flat.cc:599-604) where only rows 0 and N-1 are needed.
+__global__ void k_boundary_update(double2* __restrict__ hist, const double2* __restrict__ dp, size_t S, int M, int nz,
+                                  int opentop, const double* __restrict__ kx, const double* __restrict__ ky,
+                                  const double* __restrict__ d1r0, const double* __restrict__ d1rn) {
+  const size_t R = (size_t)3 * M;
+  for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < M; m += gridDim.x * blockDim.x) {
+    for (int c = 0; c < 3; ++c) {
+      const size_t i = (size_t)c * M + m;
+      hist[2 * R + i] = hist[0 * R + i];
+      hist[3 * R + i] = hist[1 * R + i];
+      hist[6 * R + i] = hist[4 * R + i];
+      hist[7 * R + i] = hist[5 * R + i];
+      hist[1 * R + i] = dp[(size_t)c * S + m];
+      hist[0 * R + i] = dp[(size_t)c * S + (size_t)(nz - 1) * M + m];
+    }
+    if (opentop) {
+      const double2* g = dp + 2 * S;  // dp/dz
+      double2 g0 = g[m], gn = g[(size_t)(nz - 1) * M + m];
+      double s0x = 0, s0y = 0, snx = 0, sny = 0;
+      for (int k = 0; k < nz; ++k) {
+        double2 v = g[(size_t)k * M + m];
+        s0x += d1r0[k] * v.x;
+        s0y += d1r0[k] * v.y;
+        snx += d1rn[k] * v.x;
+        sny += d1rn[k] * v.y;
+      }
+      hist[5 * R + 0 * M + m] = mul_i(kx[m], g0);
+      hist[5 * R + 1 * M + m] = mul_i(ky[m], g0);
+      hist[5 * R + 2 * M + m] = make_double2(s0x, s0y);
+      hist[4 * R + 0 * M + m] = mul_i(kx[m], gn);
+      hist[4 * R + 1 * M + m] = mul_i(ky[m], gn);
+      hist[4 * R + 2 * M + m] = make_double2(snx, sny);
+    }
+  }
+}
+void boundary_update(double2* hist, const double2* dp, size_t S, int M, int nz, int opentop, const double* kx,
+                     const double* ky, const double* d1r0, const double* d1rn, cudaStream_t s) {
+  k_boundary_update<<<nblk(M), kT, 0, s>>>(hist, dp, S, M, nz, opentop, kx, ky, d1r0, d1rn);
+  TG_LAUNCH_CHECK("k_boundary_update");
+}
+
+// projection u = u* - 2 dt c3 grad p, mean w := 0 (phase_carrier_flat.cc:609-620)
+__global__ void k_project(double2* __restrict__ U, const double2* __restrict__ SU, const double2* __restrict__ DP,
+                          size_t S, int M, double coef) {
+  const size_t n = 3 * S;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const int c = (int)(i / S);
+    const size_t e = i - (size_t)c * S;
+    double2 su = SU[i], dp = DP[i];
+    double2 u = make_double2(su.x - coef * dp.x, su.y - coef * dp.y);
+    if (c == 2 && (e % M) == 0) u = make_double2(0.0, 0.0);
+    U[i] = u;
+  }
+}
+void project(double2* U, const double2* SU, const double2* DP, size_t S, int M, double coef, cudaStream_t s) {
+  prof_begin(s, PC_ELEM, 144.0 * (double)S, 0);
+  k_project<<<nblk(3 * S), kT, 0, s>>>(U, SU, DP, S, M, coef);
+  prof_end(s);
+  TG_LAUNCH_CHECK("k_project");
+}
+
+// rows 0 and N-1 := 0 (boundary_scalar_flat.cc:150-151)
+__global__ void k_zero_rows(double2* f, int M, int nz) {
+  for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < M; m += gridDim.x * blockDim.x) {
+    f[m] = make_double2(0.0, 0.0);
+    f[(size_t)(nz - 1) * M + m] = make_double2(0.0, 0.0);
+  }
+}
+void zero_rows(double2* f, int M, int nz, cudaStream_t s) {
+  k_zero_rows<<<nblk(M), kT, 0, s>>>(f, M, nz);
+  TG_LAUNCH_CHECK("k_zero_rows");
+}
+
+// --- erosion / deposition bottom row (phase_scalar_flat.cc:340-384) ---------------
+template <typename T>
+__global__ void k_erosion_tau(const T* __restrict__ dudz, const T* __restrict__ dvdz, T* __restrict__ tau, size_t n,
+                              double re, double tauc, double rate) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    T a = dudz[i], b = dvdz[i];
+    T v = sqrt(a * a + b * b) / (T)re;
+    tau[i] = (v < (T)tauc) ? T(0) : (T)rate * (v / (T)tauc - T(1));
+  }
+}
+template <typename T>
+void erosion_tau(const T* dudz, const T* dvdz, T* tau, size_t n, double re, double tauc, double rate,
+                 cudaStream_t s) {
+  k_erosion_tau<T><<<nblk(n), kT, 0, s>>>(dudz, dvdz, tau, n, re, tauc, rate);
+  TG_LAUNCH_CHECK("k_erosion_tau");
+}
+
+__global__ void k_erosion_row(double2* __restrict__ rhs, const double2* __restrict__ ero, const double2* __restrict__ phi,
+                              int M, double wsc, double conc, double resc, double* feat) {
+  for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < M; m += gridDim.x * blockDim.x) {
+    double2 e = ero[m], p = phi[m];
+    double2 r = make_double2(e.x - wsc * p.x * conc, e.y - wsc * p.y * conc);
+    const double f = -1 * resc / conc * 10e6;
+    rhs[m] = make_double2(r.x * f, r.y * f);
+    if (m == 0) {
+      feat[28] = e.x;
+      feat[29] = wsc * p.x * conc;
+    }
+  }
+}
+void erosion_row(double2* rhs, const double2* ero, const double2* phi, int M, double wsc, double conc, double resc,
+                 double* feat, cudaStream_t s) {
+  k_erosion_row<<<nblk(M), kT, 0, s>>>(rhs, ero, phi, M, wsc, conc, resc, feat);
+  TG_LAUNCH_CHECK("k_erosion_row");
+}
+
+// --- Bartnicki positivity filter (phase_scalar_flat.cc:419-478) -----------------
+// One CTA per z plane: per-plane sums of positive, zero and negative values and
+// their counts, then the redistribution; five sweeps in one launch.
+template <typename T>
+__global__ void __launch_bounds__(1024) k_filter(T* __restrict__ phip, int plane_n) {
+  __shared__ double red[6][32];
+  __shared__ double tot[6];
+  T* p = phip + (size_t)blockIdx.x * plane_n;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int it = 0; it < 5; ++it) {
+    double a[6] = {0, 0, 0, 0, 0, 0};
+    for (int i = threadIdx.x; i < plane_n; i += blockDim.x) {
+      double v = (double)p[i];
+      if (v > 0) {
+        a[0] += v;
+        a[1] += 1;
+      } else if (v < 0) {
+        a[4] += v;
+        a[5] += 1;
+      } else {
+        a[2] += v;
+        a[3] += 1;
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      double v = a[k];
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+      if (lane == 0) red[k][warp] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 6) {
+      double s = 0;
+      for (int w = 0; w < nw; ++w) s += red[threadIdx.x][w];
+      tot[threadIdx.x] = s;
+    }
+    __syncthreads();
+    const bool kill = (tot[0] + tot[2] + tot[4]) < 0;
+    const double add = tot[1] > 0 ? tot[4] / tot[1] : 0.0;
+    for (int i = threadIdx.x; i < plane_n; i += blockDim.x) {
+      T v = p[i];
+      if (kill)
+        p[i] = T(0);
+      else
+        p[i] = (v > 0) ? (T)((double)v + add) : T(0);
+    }
+    __syncthreads();
+  }
+}
+template <typename T>
+void positivity_filter(T* phip, int plane_n, int nz, cudaStream_t s) {
+  prof_begin(s, PC_FILTER, 20.0 * sizeof(T) * (double)plane_n * nz, 0);
+  k_filter<T><<<nz, 1024, 0, s>>>(phip, plane_n);
+  prof_end(s);
+  TG_LAUNCH_CHECK("k_filter");
+}
+
+// --- features ---------------------------------------------------------------------
+// Stage-2 features of FlatCarrierPhase::Correct (phase_carrier_flat.cc:633-703).
+// bits: 10 slots of non-negative doubles reduced with atomicMax on their bit
+// patterns: 0-2 max|u_i|, 3-5 bottom plane, 6-8 top plane, 9 max CFL length.
+template <typename T>
+__global__ void k_feature_max(const T* __restrict__ unl, int nx, int ny, int nz, const double* __restrict__ glz,
+                              double lmx, double lmy, unsigned long long* bits) {
+  const size_t plane = (size_t)nx * ny, P = plane * nz;
+  double mx[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < P; i += (size_t)gridDim.x * blockDim.x) {
+    const int z = (int)(i / plane);
+    double u = fabs((double)unl[i]), v = fabs((double)unl[P + i]), w = fabs((double)unl[2 * P + i]);
+    mx[0] = fmax(mx[0], u);
+    mx[1] = fmax(mx[1], v);
+    mx[2] = fmax(mx[2], w);
+    if (z == 0) {
+      mx[3] = fmax(mx[3], u);
+      mx[4] = fmax(mx[4], v);
+      mx[5] = fmax(mx[5], w);
+    }
+    if (z == nz - 1) {
+      mx[6] = fmax(mx[6], u);
+      mx[7] = fmax(mx[7], v);
+      mx[8] = fmax(mx[8], w);
+    }
+    mx[9] = fmax(mx[9], u / lmx + v / lmy + w / glz[z]);
+  }
+#pragma unroll
+  for (int k = 0; k < 10; ++k) {
+    double v = mx[k];
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(bits + k, (unsigned long long)__double_as_longlong(v));
+  }
+}
+// flocal = feat[0..49], fglobal = feat[50..99]
+__global__ void k_feature_final(double* feat, const unsigned long long* bits, const double2* __restrict__ du, size_t S,
+                                int M, int nz) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  for (int k = 0; k < 9; ++k) feat[k] = __longlong_as_double((long long)bits[k]);
+  feat[19] = __longlong_as_double((long long)bits[9]);
+  for (int k = 0; k < 50; ++k) feat[50 + k] = feat[k];
+  // du_i/dz of the mean mode at the walls (dudxyz[i] component 2)
+  for (int i = 0; i < 3; ++i) {
+    const double2* dz = du + (size_t)(3 * i + 2) * S;
+    feat[50 + 10 + i] = dz[0].x;
+    feat[50 + 13 + i] = dz[(size_t)(nz - 1) * M].x;
+  }
+}
+template <typename T>
+void features(const T* unl, int nx, int ny, int nz, const double* glz, double lmx, double lmy,
+              unsigned long long* bits, double* feat, const double2* du, size_t S, int M, cudaStream_t s) {
+  TG_CUDA(cudaMemsetAsync(bits, 0, 10 * sizeof(unsigned long long), s));
+  size_t P = (size_t)nx * ny * nz;
+  prof_begin(s, PC_FEAT, 3.0 * sizeof(T) * (double)P, 0);
+  k_feature_max<T><<<nblk(P, 4), kT, 0, s>>>(unl, nx, ny, nz, glz, lmx, lmy, bits);
+  prof_end(s);
+  TG_LAUNCH_CHECK("k_feature_max");
+  k_feature_final<<<1, 32, 0, s>>>(feat, bits, du, S, M, nz);
+  TG_LAUNCH_CHECK("k_feature_final");
+}
+
+// trapz(gridz, real(mean column) + shift)/2 into feat[slot] (arma::trapz, used at
+// phase_carrier_flat.cc:509, phase_scalar_flat.cc:485-518)
+__global__ void k_trapz_mean(const double2* __restrict__ f, int M, int nz, const double* __restrict__ gz, double shift,
+                             double* feat, int slot) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double s = 0.0;
+  for (int k = 0; k < nz - 1; ++k)
+    s += (gz[k + 1] - gz[k]) * ((f[(size_t)k * M].x + shift) + (f[(size_t)(k + 1) * M].x + shift));
+  feat[slot] = s / 2 / 2;
+}
+void trapz_mean(const double2* f, int M, int nz, const double* gz, double shift, double* feat, int slot,
+                cudaStream_t s) {
+  k_trapz_mean<<<1, 32, 0, s>>>(f, M, nz, gz, shift, feat, slot);
+  TG_LAUNCH_CHECK("k_trapz_mean");
+}
+
+__global__ void k_set_feat(double* feat, int slot, double v) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) feat[slot] = v;
+}
+void set_feat(double* feat, int slot, double v, cudaStream_t s) {
+  k_set_feat<<<1, 32, 0, s>>>(feat, slot, v);
+  TG_LAUNCH_CHECK("k_set_feat");
+}
+
+// --- precision conversions for the mixed path --------------------------------------
+template <typename A, typename B>
+__global__ void k_convert(const A* __restrict__ a, B* __restrict__ b, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    b[i] = (B)a[i];
+}
+
+#define INST(T)                                                                                          \
+  template void products6<T>(const T*, T*, size_t, cudaStream_t);                                      \
+  template void adv_products<T>(const T*, const T*, T*, size_t, int, double, double, double, cudaStream_t); \
+  template void phi_products<T>(const T*, const T*, T*, size_t, double, double, double, cudaStream_t);  \
+  template void mul_shift<T>(const T*, const T*, T*, size_t, double, cudaStream_t);                     \
+  template void erosion_tau<T>(const T*, const T*, T*, size_t, double, double, double, cudaStream_t);   \
+  template void positivity_filter<T>(T*, int, int, cudaStream_t);                                       \
+  template void features<T>(const T*, int, int, int, const double*, double, double, unsigned long long*, \
+                            double*, const double2*, size_t, int, cudaStream_t);
+INST(double)
+INST(float)
+#undef INST
+
+}  // namespace tg

@@ -1,0 +1,40 @@
+// Launchers of the elementwise stage kernels and reductions (fields.cu).
+#pragma once
+#include "tg_common.cuh"
+
+namespace tg {
+
+void ref_to_slab(const double2* ref, double2* slab, int M, int nz, int dim, cudaStream_t s);
+void slab_to_ref(const double2* slab, double2* ref, int M, int nz, int dim, cudaStream_t s);
+
+template <typename T> void products6(const T* unl, T* prd, size_t P, cudaStream_t s);
+template <typename T>
+void adv_products(const T* unl, const T* dup, T* out, size_t P, int ncomp, double su, double sv, double sw,
+                  cudaStream_t s);
+template <typename T>
+void phi_products(const T* phip, const T* unl, T* out, size_t P, double su, double sv, double sw, cudaStream_t s);
+template <typename T> void mul_shift(const T* a, const T* b, T* out, size_t P, double sh, cudaStream_t s);
+
+void h_update(double2* H, const double2* adv, const double2* phi, size_t S, int M, double c1, double dt,
+              double bcoef, double sinsl, double cossl, int sdir, double dtf1, double dtf2, cudaStream_t s);
+void axmby(double2* y, const double2* x, size_t n, double a, double b, cudaStream_t s);
+void boundary_apply(double2* rhs, const double2* hist, size_t S, int M, int nz, double fac, double r, int opentop,
+                    double tu, double tv, double tw, cudaStream_t s);
+void boundary_update(double2* hist, const double2* dp, size_t S, int M, int nz, int opentop, const double* kx,
+                     const double* ky, const double* d1r0, const double* d1rn, cudaStream_t s);
+void project(double2* U, const double2* SU, const double2* DP, size_t S, int M, double coef, cudaStream_t s);
+void zero_rows(double2* f, int M, int nz, cudaStream_t s);
+template <typename T>
+void erosion_tau(const T* dudz, const T* dvdz, T* tau, size_t n, double re, double tauc, double rate,
+                 cudaStream_t s);
+void erosion_row(double2* rhs, const double2* ero, const double2* phi, int M, double wsc, double conc, double resc,
+                 double* feat, cudaStream_t s);
+template <typename T> void positivity_filter(T* phip, int plane_n, int nz, cudaStream_t s);
+template <typename T>
+void features(const T* unl, int nx, int ny, int nz, const double* glz, double lmx, double lmy,
+              unsigned long long* bits, double* feat, const double2* du, size_t S, int M, cudaStream_t s);
+void trapz_mean(const double2* f, int M, int nz, const double* gz, double shift, double* feat, int slot,
+                cudaStream_t s);
+void set_feat(double* feat, int slot, double v, cudaStream_t s);
+
+}  // namespace tg

@@ -1,0 +1,142 @@
+// Shared definitions of the sm_100a kernels of libturbid_gpu.so.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/turbid_gpu.h"
+
+namespace tg {
+
+// ---------------------------------------------------------------------------
+// error handling: the C ABI returns codes, the message is kept per thread
+// ---------------------------------------------------------------------------
+void set_error(const std::string& msg);
+
+struct Error {
+  int code;
+  std::string msg;
+};
+
+#define TG_CUDA(call)                                                           \
+  do {                                                                          \
+    cudaError_t e_ = (call);                                                    \
+    if (e_ != cudaSuccess)                                                      \
+      throw ::tg::Error{TG_ERR_CUDA, std::string(#call) + " > " +               \
+                                         cudaGetErrorString(e_)};               \
+  } while (0)
+
+extern long long g_launches;   // kernel launches issued by this library (host thread count)
+
+#define TG_LAUNCH_CHECK(name)                                                   \
+  do {                                                                          \
+    ++::tg::g_launches;                                                         \
+    cudaError_t e_ = cudaGetLastError();                                        \
+    if (e_ != cudaSuccess)                                                      \
+      throw ::tg::Error{TG_ERR_CUDA, std::string(name) + " launch > " +         \
+                                         cudaGetErrorString(e_)};               \
+  } while (0)
+
+// ---------------------------------------------------------------------------
+// per-kernel-class timing with CUDA events (enabled by tg_profile_begin)
+// ---------------------------------------------------------------------------
+enum ProfCat { PC_GEMM = 0, PC_FFT_FX, PC_FFT_FY, PC_FFT_BY, PC_FFT_BX, PC_ELEM, PC_FILTER, PC_FEAT, PC_N };
+void prof_begin(cudaStream_t s, int cat, double bytes, double flops);
+void prof_end(cudaStream_t s);
+
+// ---------------------------------------------------------------------------
+// complex helpers (device)
+// ---------------------------------------------------------------------------
+template <typename T> struct cplx_t;
+template <> struct cplx_t<double> { using type = double2; };
+template <> struct cplx_t<float> { using type = float2; };
+template <typename T> using cplx = typename cplx_t<T>::type;
+
+template <typename C> __host__ __device__ __forceinline__ C mkc(decltype(C::x) a, decltype(C::x) b) {
+  C r; r.x = a; r.y = b; return r;
+}
+template <typename C> __device__ __forceinline__ C cadd(C a, C b) { return mkc<C>(a.x + b.x, a.y + b.y); }
+template <typename C> __device__ __forceinline__ C csub(C a, C b) { return mkc<C>(a.x - b.x, a.y - b.y); }
+template <typename C> __device__ __forceinline__ C cmul(C a, C b) {
+  return mkc<C>(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+template <typename C> __device__ __forceinline__ C cscale(C a, decltype(C::x) s) { return mkc<C>(a.x * s, a.y * s); }
+template <typename C> __device__ __forceinline__ C cconj(C a) { return mkc<C>(a.x, -a.y); }
+
+// ---------------------------------------------------------------------------
+// FFT plan for one length (host-owned, device twiddles)
+// ---------------------------------------------------------------------------
+constexpr int kMaxPasses = 24;
+struct FftPlan {
+  int L = 0;
+  int npass = 0;
+  int rad[kMaxPasses] = {0};
+  double2* tw64 = nullptr;   // exp(-2 pi i k / L), k < L
+  float2* tw32 = nullptr;
+};
+void fft_plan_create(FftPlan& p, int L);
+void fft_plan_destroy(FftPlan& p);
+
+// Grid description the transform kernels need.
+struct TransformDims {
+  int nx, ny, nz, nxh, nyc, M;
+  const int* yidx;   // device: spectral iy -> FFT y index (P3DFFT pruning)
+};
+
+// Transforms (fft.cu).  planes = dim * nz; work = Nxh*Ny complex per plane
+// of the transform precision.
+template <typename T>
+void dft_forward(const TransformDims& d, const FftPlan& px, const FftPlan& py,
+                 const T* phys, double2* spec, int planes, void* work, cudaStream_t s);
+template <typename T>
+void dft_backward(const TransformDims& d, const FftPlan& px, const FftPlan& py,
+                  const double2* spec, T* phys, int planes, void* work, cudaStream_t s);
+
+// ---------------------------------------------------------------------------
+// z-operator GEMM (gemm.cu):  out[r][m] = epi( sum_k A[r][k] in[k][m] )
+// A: rows x K row-major FP64 with leading dimension lda (multiple of 2)
+// in/out: batch of spectral components, stride comp_stride complex each.
+// ---------------------------------------------------------------------------
+enum EpiMode {
+  EPI_STORE = 0,     // out = acc
+  EPI_RSCALE = 1,    // out = acc * R(r,m)          (Helmholtz reciprocal)
+  EPI_DIV = 2,       // out = s*(acc + i kx X0 + i ky X1)
+  EPI_LAPRHS = 3,    // out = a*c2*H + a*U - (acc + dx2*U + dy2*U)
+  EPI_GRAD = 4,      // out = acc; aux0 = i kx X; aux1 = i ky X (X = input)
+  EPI_ADDTO = 5,     // out = acc + aux0 + aux1 (three-term sums)
+};
+
+struct EpiParams {
+  int mode = EPI_STORE;
+  int nz = 0;            // number of z rows (for boundary-row rules)
+  int M = 0;
+  // EPI_RSCALE
+  const double* lam = nullptr;   // [nz]
+  const double* k2 = nullptr;    // [M]  (-kx^2 - ky^2)
+  double sigma = 0.0;
+  int null_mode = 0;             // zero R(r,0) where |lam|<1e-11 (sigma == 0)
+  // EPI_DIV / EPI_GRAD
+  const double* kx = nullptr;    // [M]
+  const double* ky = nullptr;    // [M]
+  const double2* X0 = nullptr;
+  const double2* X1 = nullptr;
+  double s = 1.0;
+  // EPI_LAPRHS
+  const double2* H = nullptr;
+  const double2* U = nullptr;
+  const double* dx2 = nullptr;   // [M]
+  const double* dy2 = nullptr;   // [M]
+  double a = 0.0, c2 = 0.0;
+  // EPI_GRAD
+  double2* aux0 = nullptr;
+  double2* aux1 = nullptr;
+  // batch strides (complex elements) for the pointers above
+  long long sX = 0, sH = 0, sU = 0, sAux = 0;
+};
+
+void zgemm_init();
+void zgemm(const double* A, int lda, int rows, int K, const double2* in, long long in_stride, double2* out,
+           long long out_stride, int M, int batch, const EpiParams& ep, cudaStream_t s);
+
+}  // namespace tg
