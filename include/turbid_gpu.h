@@ -93,7 +93,9 @@ TG_API tg_status tg_create(const tg_case* c, tg_ctx** out);
 TG_API tg_status tg_destroy(tg_ctx* ctx);
 /* dims = {nx, ny, nz, nxh, nyc, M} */
 TG_API tg_status tg_get_dims(const tg_ctx* ctx, int dims[6]);
-/* Use a caller's CUDA stream (cudaStream_t passed as void*); NULL = own stream. */
+/* Order all later work of the context on the caller's CUDA stream
+ * (cudaStream_t passed as void*, used verbatim: NULL is the legacy default
+ * stream).  The library's own stream, created by tg_create, is released. */
 TG_API tg_status tg_set_stream(tg_ctx* ctx, void* stream);
 TG_API tg_status tg_synchronize(tg_ctx* ctx);
 

@@ -23,7 +23,11 @@ CASE_KEYS = ("nx", "ny", "nz", "lx", "ly", "nphase", "mapping", "mapping_coef", 
 
 
 def gpu_case(cfg: O.CaseConfig, precision="fp64") -> tb.ChannelCase:
-    return tb.ChannelCase(precision=precision, **{k: getattr(cfg, k) for k in CASE_KEYS})
+    """A case whose work is ordered on torch's current stream (the primitives are asynchronous)."""
+    import torch
+    gc = tb.ChannelCase(precision=precision, **{k: getattr(cfg, k) for k in CASE_KEYS})
+    gc.set_stream(torch.cuda.current_stream().cuda_stream)
+    return gc
 
 
 def install_oracle_decompositions(gc, sol):

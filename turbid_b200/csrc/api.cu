@@ -822,14 +822,9 @@ tg_status tg_set_stream(tg_ctx* ctx, void* stream) {
   Ctx& x = *reinterpret_cast<Ctx*>(ctx);
   TG_TRY({
     TG_CUDA(cudaStreamSynchronize(x.s));
-    if (stream) {
-      if (x.own_stream) cudaStreamDestroy(x.s);
-      x.s = reinterpret_cast<cudaStream_t>(stream);
-      x.own_stream = false;
-    } else if (!x.own_stream) {
-      TG_CUDA(cudaStreamCreateWithFlags(&x.s, cudaStreamNonBlocking));
-      x.own_stream = true;
-    }
+    if (x.own_stream) TG_CUDA(cudaStreamDestroy(x.s));
+    x.s = reinterpret_cast<cudaStream_t>(stream);
+    x.own_stream = false;
   });
 }
 

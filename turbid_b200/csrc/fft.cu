@@ -146,6 +146,111 @@ __device__ cplx<T>* fft_batch(cplx<T>* b0, cplx<T>* b1, int NB, const PlanArgs& 
   return in;
 }
 
+// ---------------------------------------------------------------------------
+// compile-time Stockham passes for power-of-two lengths: radix-16 passes
+// while 16 divides the remaining length, then one radix-8/4/2 pass; the small
+// DFTs are even/odd splits with constant twiddles, all indexing constant-folded.
+// ---------------------------------------------------------------------------
+template <typename C, int DIR>
+__device__ __forceinline__ C rot(C a, double c, double s) {  // a * (c + i DIR s)
+  using R = decltype(C::x);
+  const R cr = (R)c, sr = (R)(DIR * s);
+  return mkc<C>(a.x * cr - a.y * sr, a.x * sr + a.y * cr);
+}
+
+// cos(2 pi i / 16); sin(2 pi i / 16) = cos16(i - 4)
+__host__ __device__ constexpr double cos16(int i) {
+  i &= 15;
+  if (i > 8) i = 16 - i;
+  return i == 0 ? 1.0
+       : i == 1 ? 0.92387953251128675613
+       : i == 2 ? 0.70710678118654752440
+       : i == 3 ? 0.38268343236508977173
+       : i == 4 ? 0.0
+       : i == 5 ? -0.38268343236508977173
+       : i == 6 ? -0.70710678118654752440
+       : i == 7 ? -0.92387953251128675613
+       : -1.0;
+}
+
+template <int R, int DIR, typename C>
+__device__ __forceinline__ void dft_ct(C* v) {
+  if constexpr (R == 1) {
+    return;
+  } else if constexpr (R == 2) {
+    C a = v[0], b = v[1];
+    v[0] = cadd(a, b);
+    v[1] = csub(a, b);
+  } else {
+    constexpr int H = R / 2;
+    C e[H], o[H];
+#pragma unroll
+    for (int m = 0; m < H; ++m) {
+      e[m] = v[2 * m];
+      o[m] = v[2 * m + 1];
+    }
+    dft_ct<H, DIR>(e);
+    dft_ct<H, DIR>(o);
+#pragma unroll
+    for (int k = 0; k < H; ++k) {
+      // W_R^k = cos(2 pi k/R) + i DIR sin(2 pi k/R) with DIR = -1 forward (R <= 16)
+      const int i16 = k * (16 / R);
+      C t;
+      if (k == 0) {
+        t = o[k];
+      } else if (4 * k == R) {
+        t = (DIR < 0) ? mkc<C>(o[k].y, -o[k].x) : mkc<C>(-o[k].y, o[k].x);
+      } else {
+        t = rot<C, DIR>(o[k], cos16(i16), cos16(i16 - 4));
+      }
+      v[k] = cadd(e[k], t);
+      v[k + H] = csub(e[k], t);
+    }
+  }
+}
+
+template <typename T, int DIR, int L, int Ns>
+__device__ __forceinline__ cplx<T>* ct_passes(cplx<T>* in, cplx<T>* out, int NB, const cplx<T>* __restrict__ tw) {
+  using C = cplx<T>;
+  if constexpr (Ns >= L) {
+    return in;
+  } else {
+    constexpr int rem = L / Ns;
+    constexpr int R = rem >= 16 ? 16 : rem;
+    constexpr int nb = L / R;
+    constexpr int twstep = L / (Ns * R);
+    for (int idx = threadIdx.x; idx < NB * nb; idx += blockDim.x) {
+      const int b = idx / nb;
+      const int j = idx - b * nb;
+      const C* src = in + b * L;
+      C* dst = out + b * L;
+      const int jm = j % Ns;
+      const int base = (j - jm) * R + jm;
+      C v[R];
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        v[r] = src[j + r * nb];
+        if (Ns > 1 && r > 0) v[r] = cmul(v[r], tw_get<T, DIR>(tw, jm * r * twstep));
+      }
+      dft_ct<R, DIR>(v);
+#pragma unroll
+      for (int k = 0; k < R; ++k) dst[base + k * Ns] = v[k];
+    }
+    __syncthreads();
+    return ct_passes<T, DIR, L, Ns * R>(out, in, NB, tw);
+  }
+}
+
+// FFT of NB length-L transforms in shared memory; LC = L at compile time or 0
+template <typename T, int DIR, int LC>
+__device__ __forceinline__ cplx<T>* fft_any(cplx<T>* b0, cplx<T>* b1, int NB, const PlanArgs& pl,
+                                            const cplx<T>* __restrict__ tw) {
+  if constexpr (LC > 0)
+    return ct_passes<T, DIR, LC, 1>(b0, b1, NB, tw);
+  else
+    return fft_batch<T, DIR>(b0, b1, NB, pl, tw);
+}
+
 template <typename T> struct Tw;
 template <> struct Tw<double> {
   static __host__ const double2* get(const FftPlan& p) { return p.tw64; }
@@ -157,14 +262,14 @@ template <> struct Tw<float> {
 // ---------------------------------------------------------------------------
 // forward x pass: phys [plane][y][x] (T) -> work [plane][kx][y] (cplx<T>)
 // ---------------------------------------------------------------------------
-template <typename T>
+template <typename T, int LC>
 __global__ void __launch_bounds__(256) fwd_x_kernel(TransformDims d, PlanArgs pl, const cplx<T>* __restrict__ tw,
                                                     const T* __restrict__ phys, cplx<T>* __restrict__ work, int NB) {
   using C = cplx<T>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* b0 = reinterpret_cast<C*>(smem_raw);
-  C* b1 = b0 + NB * pl.L;
-  const int L = pl.L;  // == nx
+  C* b1 = b0 + NB * (LC > 0 ? LC : pl.L);
+  const int L = LC > 0 ? LC : pl.L;  // == nx
   const int plane = blockIdx.y;
   const int y0 = blockIdx.x * 2 * NB;
   const T* src = phys + (size_t)plane * d.ny * d.nx;
@@ -176,7 +281,7 @@ __global__ void __launch_bounds__(256) fwd_x_kernel(TransformDims d, PlanArgs pl
     b0[idx] = mkc<C>(re, im);
   }
   __syncthreads();
-  C* r = fft_batch<T, -1>(b0, b1, NB, pl, tw);
+  C* r = fft_any<T, -1, LC>(b0, b1, NB, pl, tw);
   const int rows = 2 * NB;
   C* dst = work + (size_t)plane * d.nxh * d.ny;
   for (int idx = threadIdx.x; idx < rows * d.nxh; idx += blockDim.x) {
@@ -198,15 +303,15 @@ __global__ void __launch_bounds__(256) fwd_x_kernel(TransformDims d, PlanArgs pl
 }
 
 // forward y pass: work [plane][kx][y] -> spec [plane][iy + nyc*kx] (double2)
-template <typename T>
+template <typename T, int LC>
 __global__ void __launch_bounds__(256) fwd_y_kernel(TransformDims d, PlanArgs pl, const cplx<T>* __restrict__ tw,
                                                     const cplx<T>* __restrict__ work, double2* __restrict__ spec,
                                                     int NB, double scale) {
   using C = cplx<T>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* b0 = reinterpret_cast<C*>(smem_raw);
-  C* b1 = b0 + NB * pl.L;
-  const int L = pl.L;  // == ny
+  C* b1 = b0 + NB * (LC > 0 ? LC : pl.L);
+  const int L = LC > 0 ? LC : pl.L;  // == ny
   const int plane = blockIdx.y;
   const int k0 = blockIdx.x * NB;
   const C* src = work + (size_t)plane * d.nxh * d.ny;
@@ -216,7 +321,7 @@ __global__ void __launch_bounds__(256) fwd_y_kernel(TransformDims d, PlanArgs pl
     b0[idx] = k < d.nxh ? src[(size_t)k * d.ny + y] : mkc<C>(0, 0);
   }
   __syncthreads();
-  C* r = fft_batch<T, -1>(b0, b1, NB, pl, tw);
+  C* r = fft_any<T, -1, LC>(b0, b1, NB, pl, tw);
   double2* dst = spec + (size_t)plane * d.M;
   for (int idx = threadIdx.x; idx < NB * d.nyc; idx += blockDim.x) {
     const int c = idx / d.nyc, iy = idx - c * d.nyc;
@@ -228,15 +333,15 @@ __global__ void __launch_bounds__(256) fwd_y_kernel(TransformDims d, PlanArgs pl
 }
 
 // backward y pass: spec -> work (zero-filled pruned modes, unscaled)
-template <typename T>
+template <typename T, int LC>
 __global__ void __launch_bounds__(256) bwd_y_kernel(TransformDims d, PlanArgs pl, const cplx<T>* __restrict__ tw,
                                                     const double2* __restrict__ spec, cplx<T>* __restrict__ work,
                                                     int NB) {
   using C = cplx<T>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* b0 = reinterpret_cast<C*>(smem_raw);
-  C* b1 = b0 + NB * pl.L;
-  const int L = pl.L;  // == ny
+  C* b1 = b0 + NB * (LC > 0 ? LC : pl.L);
+  const int L = LC > 0 ? LC : pl.L;  // == ny
   const int plane = blockIdx.y;
   const int k0 = blockIdx.x * NB;
   for (int idx = threadIdx.x; idx < NB * L; idx += blockDim.x) b0[idx] = mkc<C>(0, 0);
@@ -250,7 +355,7 @@ __global__ void __launch_bounds__(256) bwd_y_kernel(TransformDims d, PlanArgs pl
     b0[c * L + d.yidx[iy]] = mkc<C>((T)v.x, (T)v.y);
   }
   __syncthreads();
-  C* r = fft_batch<T, +1>(b0, b1, NB, pl, tw);
+  C* r = fft_any<T, +1, LC>(b0, b1, NB, pl, tw);
   C* dst = work + (size_t)plane * d.nxh * d.ny;
   for (int idx = threadIdx.x; idx < NB * L; idx += blockDim.x) {
     const int c = idx / L, y = idx - c * L;
@@ -261,14 +366,14 @@ __global__ void __launch_bounds__(256) bwd_y_kernel(TransformDims d, PlanArgs pl
 
 // backward x pass: work [plane][kx][y] -> phys [plane][y][x]; two rows per
 // complex FFT; the imaginary part of the kx = 0 coefficient is ignored (c2r).
-template <typename T>
+template <typename T, int LC>
 __global__ void __launch_bounds__(256) bwd_x_kernel(TransformDims d, PlanArgs pl, const cplx<T>* __restrict__ tw,
                                                     const cplx<T>* __restrict__ work, T* __restrict__ phys, int NB) {
   using C = cplx<T>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* b0 = reinterpret_cast<C*>(smem_raw);
-  C* b1 = b0 + NB * pl.L;
-  const int L = pl.L;  // == nx
+  C* b1 = b0 + NB * (LC > 0 ? LC : pl.L);
+  const int L = LC > 0 ? LC : pl.L;  // == nx
   const int plane = blockIdx.y;
   const int y0 = blockIdx.x * 2 * NB;
   for (int idx = threadIdx.x; idx < NB * L; idx += blockDim.x) b0[idx] = mkc<C>(0, 0);
@@ -288,7 +393,7 @@ __global__ void __launch_bounds__(256) bwd_x_kernel(TransformDims d, PlanArgs pl
     if (k > 0) b0[p * L + (L - k)] = mkc<C>(h1.x + h2.y, -h1.y + h2.x);
   }
   __syncthreads();
-  C* r = fft_batch<T, +1>(b0, b1, NB, pl, tw);
+  C* r = fft_any<T, +1, LC>(b0, b1, NB, pl, tw);
   T* dst = phys + (size_t)plane * d.ny * d.nx;
   for (int idx = threadIdx.x; idx < NB * L; idx += blockDim.x) {
     const int p = idx / L, x = idx - p * L;
@@ -314,20 +419,43 @@ static int pick_nb(int L, size_t csize) {
   return nb;
 }
 
+// lengths with a compile-time specialisation (powers of two); others use LC = 0
+#define TG_FFT_LENGTHS(X) X(8) X(16) X(32) X(64) X(128) X(256) X(512) X(1024)
+
+#define TG_FFT_DISPATCH(L, CALL)          \
+  switch (L) {                            \
+    case 8: CALL(8); break;               \
+    case 16: CALL(16); break;             \
+    case 32: CALL(32); break;             \
+    case 64: CALL(64); break;             \
+    case 128: CALL(128); break;           \
+    case 256: CALL(256); break;           \
+    case 512: CALL(512); break;           \
+    case 1024: CALL(1024); break;         \
+    default: CALL(0); break;              \
+  }
+
 template <typename Kern>
 static void set_smem(Kern k) {
   TG_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFftSmemBudget));
 }
 
+template <typename T, int LC>
+static void set_smem_all() {
+  set_smem(fwd_x_kernel<T, LC>);
+  set_smem(fwd_y_kernel<T, LC>);
+  set_smem(bwd_y_kernel<T, LC>);
+  set_smem(bwd_x_kernel<T, LC>);
+}
+
 void fft_init() {
-  set_smem(fwd_x_kernel<double>);
-  set_smem(fwd_y_kernel<double>);
-  set_smem(bwd_y_kernel<double>);
-  set_smem(bwd_x_kernel<double>);
-  set_smem(fwd_x_kernel<float>);
-  set_smem(fwd_y_kernel<float>);
-  set_smem(bwd_y_kernel<float>);
-  set_smem(bwd_x_kernel<float>);
+#define TG_INIT_L(L)          \
+  set_smem_all<double, L>(); \
+  set_smem_all<float, L>();
+  TG_FFT_LENGTHS(TG_INIT_L)
+#undef TG_INIT_L
+  set_smem_all<double, 0>();
+  set_smem_all<float, 0>();
 }
 
 template <typename T>
@@ -339,8 +467,12 @@ void dft_forward(const TransformDims& d, const FftPlan& px, const FftPlan& py, c
     int nb = pick_nb(px.L, sizeof(C));
     size_t sm = 2 * (size_t)nb * px.L * sizeof(C);
     dim3 grid((d.ny + 2 * nb - 1) / (2 * nb), planes);
+    const PlanArgs pa = plan_args(px);
+    const C* tw = Tw<T>::get(px);
     prof_begin(s, PC_FFT_FX, (double)planes * d.ny * (d.nx * sizeof(T) + d.nxh * sizeof(C)), 0);
-    fwd_x_kernel<T><<<grid, 256, sm, s>>>(d, plan_args(px), Tw<T>::get(px), phys, w, nb);
+#define TG_CALL(LC) fwd_x_kernel<T, LC><<<grid, 256, sm, s>>>(d, pa, tw, phys, w, nb)
+    TG_FFT_DISPATCH(px.L, TG_CALL)
+#undef TG_CALL
     prof_end(s);
     TG_LAUNCH_CHECK("fwd_x_kernel");
   }
@@ -348,9 +480,13 @@ void dft_forward(const TransformDims& d, const FftPlan& px, const FftPlan& py, c
     int nb = pick_nb(py.L, sizeof(C));
     size_t sm = 2 * (size_t)nb * py.L * sizeof(C);
     dim3 grid((d.nxh + nb - 1) / nb, planes);
+    const PlanArgs pa = plan_args(py);
+    const C* tw = Tw<T>::get(py);
+    const double scale = 1.0 / ((double)d.nx * (double)d.ny);
     prof_begin(s, PC_FFT_FY, (double)planes * ((double)d.nxh * d.ny * sizeof(C) + (double)d.M * sizeof(double2)), 0);
-    fwd_y_kernel<T><<<grid, 256, sm, s>>>(d, plan_args(py), Tw<T>::get(py), w, spec, nb,
-                                          1.0 / ((double)d.nx * (double)d.ny));
+#define TG_CALL(LC) fwd_y_kernel<T, LC><<<grid, 256, sm, s>>>(d, pa, tw, w, spec, nb, scale)
+    TG_FFT_DISPATCH(py.L, TG_CALL)
+#undef TG_CALL
     prof_end(s);
     TG_LAUNCH_CHECK("fwd_y_kernel");
   }
@@ -365,8 +501,12 @@ void dft_backward(const TransformDims& d, const FftPlan& px, const FftPlan& py, 
     int nb = pick_nb(py.L, sizeof(C));
     size_t sm = 2 * (size_t)nb * py.L * sizeof(C);
     dim3 grid((d.nxh + nb - 1) / nb, planes);
+    const PlanArgs pa = plan_args(py);
+    const C* tw = Tw<T>::get(py);
     prof_begin(s, PC_FFT_BY, (double)planes * ((double)d.nxh * d.ny * sizeof(C) + (double)d.M * sizeof(double2)), 0);
-    bwd_y_kernel<T><<<grid, 256, sm, s>>>(d, plan_args(py), Tw<T>::get(py), spec, w, nb);
+#define TG_CALL(LC) bwd_y_kernel<T, LC><<<grid, 256, sm, s>>>(d, pa, tw, spec, w, nb)
+    TG_FFT_DISPATCH(py.L, TG_CALL)
+#undef TG_CALL
     prof_end(s);
     TG_LAUNCH_CHECK("bwd_y_kernel");
   }
@@ -374,8 +514,12 @@ void dft_backward(const TransformDims& d, const FftPlan& px, const FftPlan& py, 
     int nb = pick_nb(px.L, sizeof(C));
     size_t sm = 2 * (size_t)nb * px.L * sizeof(C);
     dim3 grid((d.ny + 2 * nb - 1) / (2 * nb), planes);
+    const PlanArgs pa = plan_args(px);
+    const C* tw = Tw<T>::get(px);
     prof_begin(s, PC_FFT_BX, (double)planes * d.ny * (d.nx * sizeof(T) + d.nxh * sizeof(C)), 0);
-    bwd_x_kernel<T><<<grid, 256, sm, s>>>(d, plan_args(px), Tw<T>::get(px), w, phys, nb);
+#define TG_CALL(LC) bwd_x_kernel<T, LC><<<grid, 256, sm, s>>>(d, pa, tw, w, phys, nb)
+    TG_FFT_DISPATCH(px.L, TG_CALL)
+#undef TG_CALL
     prof_end(s);
     TG_LAUNCH_CHECK("bwd_x_kernel");
   }
