@@ -179,6 +179,23 @@ TG_API tg_status tg_profile_end(tg_ctx* ctx, int ncat, double* ms, double* bytes
  * y c2c, scaled 1/(NxNy).  phys: dim physical fields; spec: dim spectral. */
 TG_API tg_status tg_dft_forward_f64(tg_ctx* ctx, const double* phys, double* spec, int dim);
 TG_API tg_status tg_dft_forward_f32(tg_ctx* ctx, const float* phys, double* spec, int dim);
+/* Allocation-free variant of tg_dft_forward_f64 (no counterpart in the
+ * reference).  For callers that must not allocate device memory: a host code
+ * that reserves and manages all device memory itself (a solver sized to fill
+ * HBM with its own fields, or one that runs under a fixed memory budget),
+ * where a cudaMalloc would fail or take memory the caller has promised
+ * elsewhere.  It needs no tg_ctx (tg_create allocates): phys and spec are the
+ * caller's device buffers in the layouts above, stream is a cudaStream_t
+ * (NULL = legacy default stream).  The x->y intermediate lives in a 16 MiB
+ * device array inside the library (every GPU that loads the library holds it
+ * until exit), so nx and ny must be powers of two in [8, 1024]; larger grids
+ * are rejected with TG_ERR_SHAPE.  The first call on each device sets up the
+ * static twiddle and index tables on that device (make it with the device
+ * current).  All calls share the one scratch array: calls whose work overlaps
+ * on the GPU (other streams or other host threads) race; order them on one
+ * stream.  Results equal tg_dft_forward_f64's. */
+TG_API tg_status tg_dft_forward_f64_noalloc(int nx, int ny, int nz, const double* phys,
+                                            double* spec, int dim, void* stream);
 /* RealCplxCube::DftBackward (src/cube_real_cplx.cc:542-555): zero-fill, unscaled. */
 TG_API tg_status tg_dft_backward_f64(tg_ctx* ctx, const double* spec, double* phys, int dim);
 TG_API tg_status tg_dft_backward_f32(tg_ctx* ctx, const double* spec, float* phys, int dim);

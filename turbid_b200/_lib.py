@@ -94,6 +94,7 @@ _SIGS = [
     ("tg_profile_end", _c_i, [_vp, _c_i, _pd, _pd, _pd, _pi]),
     ("tg_dft_forward_f64", _c_i, [_vp, _vp, _vp, _c_i]),
     ("tg_dft_forward_f32", _c_i, [_vp, _vp, _vp, _c_i]),
+    ("tg_dft_forward_f64_noalloc", _c_i, [_c_i, _c_i, _c_i, _vp, _vp, _c_i, _vp]),
     ("tg_dft_backward_f64", _c_i, [_vp, _vp, _vp, _c_i]),
     ("tg_dft_backward_f32", _c_i, [_vp, _vp, _vp, _c_i]),
     ("tg_multiply", _c_i, [_vp, _pd, _vp, _vp, _c_i]),

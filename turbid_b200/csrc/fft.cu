@@ -10,8 +10,10 @@
 //           wavenumbers kept (kx-major), scaled by 1/(Nx*Ny).
 // The 1-D FFTs are mixed-radix Stockham passes in shared memory with
 // twiddles from a table computed once per length on the host.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 
 #include "tg_common.cuh"
 
@@ -535,3 +537,143 @@ template void dft_backward<float>(const TransformDims&, const FftPlan&, const Ff
                                   void*, cudaStream_t);
 
 }  // namespace tg
+
+// ===========================================================================
+// Allocation-free forward transform: tg_dft_forward_f64_noalloc.
+//
+// Same kernels, twiddles and pruning as tg_dft_forward_f64, but nothing is
+// allocated: the x->y intermediate lives in a file-scope device array, and
+// the twiddle tables / y-index maps of every supported length are written
+// once per device into file-scope device arrays.  Host code must not use the
+// arrays' names as device addresses (they are host-side stand-ins); their
+// device addresses are taken with cudaGetSymbolAddress in the per-device
+// set-up below.
+// ===========================================================================
+namespace tg {
+namespace {
+constexpr size_t kNoAllocScratch = size_t(1) << 20;   // double2 elements = 16 MiB
+constexpr int kNoAllocMinL = 8, kNoAllocMaxL = 1024;  // power-of-two lengths
+constexpr int kNoAllocTable = 2 * kNoAllocMaxL;       // sum of all supported lengths
+__device__ __align__(256) double2 g_noalloc_scratch[kNoAllocScratch];
+__device__ __align__(256) double2 g_noalloc_tw[kNoAllocTable];
+__device__ __align__(256) int g_noalloc_yidx[kNoAllocTable];
+
+struct NoAllocDevice {
+  bool ready = false;
+  double2* scratch = nullptr;
+  double2* tw = nullptr;
+  int* yidx = nullptr;
+};
+constexpr int kNoAllocMaxDevices = 64;
+NoAllocDevice g_noalloc_dev[kNoAllocMaxDevices];
+std::mutex g_noalloc_mu;
+
+// table offset of length L: 8 + 16 + ... + L/2 == L - 8
+inline int noalloc_offset(int L) { return L - kNoAllocMinL; }
+
+bool is_supported_pow2(int L) { return L >= kNoAllocMinL && L <= kNoAllocMaxL && (L & (L - 1)) == 0; }
+
+// Per-device set-up, run by the first call on each device (device current).
+NoAllocDevice& noalloc_setup() {
+  int dev = 0;
+  TG_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kNoAllocMaxDevices) throw Error{TG_ERR_ARG, "tg_dft_forward_f64_noalloc > device index out of range"};
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  NoAllocDevice& d = g_noalloc_dev[dev];
+  if (d.ready) return d;
+  std::vector<double2> tw(kNoAllocTable, make_double2(0.0, 0.0));
+  std::vector<int> ym(kNoAllocTable, 0);
+  for (int L = kNoAllocMinL; L <= kNoAllocMaxL; L *= 2) {
+    const int off = noalloc_offset(L);
+    for (int k = 0; k < L; ++k) {  // same evaluation as fft_plan_create
+      long double a = -2.0L * 3.141592653589793238462643383279502884L * (long double)k / (long double)L;
+      tw[off + k] = make_double2((double)cosl(a), (double)sinl(a));
+    }
+    const int nyc = L / 3 * 2, h = nyc / 2;
+    for (int iy = 0; iy < nyc; ++iy) ym[off + iy] = iy < h ? iy : L - (nyc - iy);
+  }
+  TG_CUDA(cudaMemcpyToSymbol(g_noalloc_tw, tw.data(), sizeof(double2) * kNoAllocTable));
+  TG_CUDA(cudaMemcpyToSymbol(g_noalloc_yidx, ym.data(), sizeof(int) * kNoAllocTable));
+  TG_CUDA(cudaGetSymbolAddress((void**)&d.scratch, g_noalloc_scratch));
+  TG_CUDA(cudaGetSymbolAddress((void**)&d.tw, g_noalloc_tw));
+  TG_CUDA(cudaGetSymbolAddress((void**)&d.yidx, g_noalloc_yidx));
+  set_smem_all<double, 0>();
+#define TG_INIT_L(L) set_smem_all<double, L>();
+  TG_FFT_LENGTHS(TG_INIT_L)
+#undef TG_INIT_L
+  d.ready = true;
+  return d;
+}
+
+PlanArgs pow2_plan(int L) {
+  PlanArgs a{};
+  a.L = L;
+  a.npass = 0;
+  int n = L;
+  while (n % 4 == 0) {
+    a.rad[a.npass++] = 4;
+    n /= 4;
+  }
+  while (n % 2 == 0) {
+    a.rad[a.npass++] = 2;
+    n /= 2;
+  }
+  return a;
+}
+
+void noalloc_forward(int nx, int ny, int nz, const double* phys, double* spec, int dim, cudaStream_t s) {
+  if (!is_supported_pow2(nx) || !is_supported_pow2(ny))
+    throw Error{TG_ERR_SHAPE, "tg_dft_forward_f64_noalloc > nx and ny must be powers of two in [8, 1024]"};
+  if (nz < 1 || dim < 1) throw Error{TG_ERR_SHAPE, "tg_dft_forward_f64_noalloc > nz and dim must be positive"};
+  if (!phys || !spec) throw Error{TG_ERR_ARG, "tg_dft_forward_f64_noalloc > null field pointer"};
+  NoAllocDevice& dv = noalloc_setup();
+  TransformDims d{};
+  d.nx = nx;
+  d.ny = ny;
+  d.nz = nz;
+  d.nxh = nx / 3 * 2 / 2 + 1;
+  d.nyc = ny / 3 * 2;
+  d.M = d.nyc * d.nxh;
+  d.yidx = dv.yidx + noalloc_offset(ny);
+  const size_t plane_work = (size_t)d.nxh * ny;   // x->y intermediate per plane
+  const int chunk = (int)(kNoAllocScratch / plane_work);
+  if (chunk < 1) throw Error{TG_ERR_SHAPE, "tg_dft_forward_f64_noalloc > plane larger than the static scratch"};
+  const PlanArgs pax = pow2_plan(nx), pay = pow2_plan(ny);
+  const double2* twx = dv.tw + noalloc_offset(nx);
+  const double2* twy = dv.tw + noalloc_offset(ny);
+  const int nbx = pick_nb(nx, sizeof(double2)), nby = pick_nb(ny, sizeof(double2));
+  const size_t smx = 2 * (size_t)nbx * nx * sizeof(double2), smy = 2 * (size_t)nby * ny * sizeof(double2);
+  const double scale = 1.0 / ((double)nx * (double)ny);
+  const int planes = dim * nz;
+  for (int p0 = 0; p0 < planes; p0 += chunk) {
+    const int np = std::min(chunk, planes - p0);
+    const double* in = phys + (size_t)p0 * nx * ny;
+    double2* out = reinterpret_cast<double2*>(spec) + (size_t)p0 * d.M;
+    dim3 gx((ny + 2 * nbx - 1) / (2 * nbx), np), gy((d.nxh + nby - 1) / nby, np);
+#define TG_CALL(LC) fwd_x_kernel<double, LC><<<gx, 256, smx, s>>>(d, pax, twx, in, dv.scratch, nbx)
+    TG_FFT_DISPATCH(nx, TG_CALL)
+#undef TG_CALL
+    TG_LAUNCH_CHECK("fwd_x_kernel (noalloc)");
+#define TG_CALL(LC) fwd_y_kernel<double, LC><<<gy, 256, smy, s>>>(d, pay, twy, dv.scratch, out, nby, scale)
+    TG_FFT_DISPATCH(ny, TG_CALL)
+#undef TG_CALL
+    TG_LAUNCH_CHECK("fwd_y_kernel (noalloc)");
+  }
+}
+}  // namespace
+
+}  // namespace tg
+
+extern "C" TG_API tg_status tg_dft_forward_f64_noalloc(int nx, int ny, int nz, const double* phys, double* spec,
+                                                       int dim, void* stream) {
+  try {
+    tg::noalloc_forward(nx, ny, nz, phys, spec, dim, reinterpret_cast<cudaStream_t>(stream));
+    return TG_OK;
+  } catch (const tg::Error& e) {
+    tg::set_error(e.msg);
+    return e.code;
+  } catch (const std::exception& e) {
+    tg::set_error(e.what());
+    return TG_ERR_CUDA;
+  }
+}
