@@ -88,10 +88,7 @@ struct Ctx {
   double *kx = nullptr, *ky = nullptr, *dx2 = nullptr, *dy2 = nullptr, *k2 = nullptr;
   double *gz = nullptr, *glz = nullptr, *d1r0 = nullptr, *d1rn = nullptr;
   int* yidx = nullptr;
-  double *D1p = nullptr, *D2p = nullptr, *Atmp = nullptr;
-  int lda = 0, rowsPad = 0;
-  double* Einvf[5] = {nullptr};
-  double* Ef[5] = {nullptr};
+  ZOperator opD1, opD2, opTmp, opEinv[5], opE[5];
   double* lamd[5] = {nullptr};
   FftPlan px, py;
   TransformDims td{};
@@ -138,18 +135,16 @@ struct Ctx {
 // ---------------------------------------------------------------------------
 // construction
 // ---------------------------------------------------------------------------
-static void upload_padded(Ctx& x, double* dst, const std::vector<double>& A) {
-  std::vector<double> pad((size_t)x.rowsPad * x.lda, 0.0);
-  for (int i = 0; i < x.nz; ++i)
-    for (int j = 0; j < x.nz; ++j) pad[(size_t)i * x.lda + j] = A[(size_t)i * x.nz + j];
-  TG_CUDA(cudaMemcpy(dst, pad.data(), pad.size() * sizeof(double), cudaMemcpyHostToDevice));
+static std::function<double*(size_t)> allocator(Ctx& x) {
+  return [&x](size_t n) { return x.dalloc<double>(n); };
 }
 
 static void install_decomposition(Ctx& x, int which) {
   std::vector<double> Ei, E;
   fold_decomposition(x.dec[which], which == 3, Ei, E);
-  upload_padded(x, x.Einvf[which], Ei);
-  upload_padded(x, x.Ef[which], E);
+  zop_build(x.opEinv[which], Ei, x.nz, false, allocator(x));
+  zop_build(x.opE[which], E, x.nz, false, allocator(x));
+  if (!x.lamd[which]) x.lamd[which] = x.dalloc<double>(x.nz);
   TG_CUDA(cudaMemcpy(x.lamd[which], x.dec[which].lam.data(), sizeof(double) * x.nz, cudaMemcpyHostToDevice));
 }
 
@@ -243,15 +238,10 @@ static Ctx* create(const tg_case& c) {
   TG_CUDA(cudaMemcpy(x.d1rn, x.D1h.data() + (size_t)(x.nz - 1) * x.nz, sizeof(double) * x.nz,
                      cudaMemcpyHostToDevice));
 
-  // operators (padded for the GEMM tiles)
-  x.lda = (x.nz + 15) / 16 * 16;
-  x.rowsPad = (x.nz + 63) / 64 * 64;
-  const size_t opsz = (size_t)x.rowsPad * x.lda;
-  x.D1p = x.dalloc<double>(opsz);
-  x.D2p = x.dalloc<double>(opsz);
-  x.Atmp = x.dalloc<double>(opsz);
-  upload_padded(x, x.D1p, x.D1h);
-  upload_padded(x, x.D2p, x.D2h);
+  // operators: dense copies, plus folded halves for the centro-(anti)symmetric
+  // derivative matrices (the Chebyshev grid is symmetric about z = 0)
+  zop_build(x.opD1, x.D1h, x.nz, true, allocator(x));
+  zop_build(x.opD2, x.D2h, x.nz, true, allocator(x));
   // decompositions: u, v, w, p (phase_carrier_flat.cc:186-201), scalar (phase_scalar_flat.cc:186-200)
   const double* bcs[4] = {c.bc_u, c.bc_v, c.bc_w, c.bc_p};
   for (int s = 0; s < 3; ++s) x.sig_u[s] = -c.reynolds / c.dt / RK3[2][s];
@@ -273,9 +263,6 @@ static Ctx* create(const tg_case& c) {
     } catch (std::exception& e) {
       throw Error{TG_ERR_SETUP, std::string("CmDz2DecompositionCplx::Construct > ") + e.what()};
     }
-    x.Einvf[w] = x.dalloc<double>(opsz);
-    x.Ef[w] = x.dalloc<double>(opsz);
-    x.lamd[w] = x.dalloc<double>(x.nz);
     install_decomposition(x, w);
   }
 
@@ -330,11 +317,11 @@ static Ctx* create(const tg_case& c) {
 // ---------------------------------------------------------------------------
 // helpers
 // ---------------------------------------------------------------------------
-static void gemm(Ctx& x, const double* A, const double2* in, long long sin, double2* out, long long sout, int batch,
-                 EpiParams ep) {
+static void gemm(Ctx& x, const ZOperator& A, const double2* in, long long sin, double2* out, long long sout,
+                 int batch, EpiParams ep) {
   ep.nz = x.nz;
   ep.M = x.M;
-  zgemm(A, x.lda, x.nz, x.nz, in, sin, out, sout, x.M, batch, ep, x.s);
+  zgemm(A, in, sin, out, sout, x.M, batch, ep, x.s);
 }
 
 template <typename T>
@@ -416,7 +403,7 @@ static void carrier_predict(Ctx& x, int stage) {
     ep.aux0 = x.DU;
     ep.aux1 = x.DU + S;
     ep.sAux = 3 * S;
-    gemm(x, x.D1p, x.U, S, x.DU + 2 * S, 3 * S, 3, ep);
+    gemm(x, x.opD1, x.U, S, x.DU + 2 * S, 3 * S, 3, ep);
   };
   // NonlinearVelocity (phase_carrier_flat.cc:716-813)
   if (x.alternation) {
@@ -432,9 +419,10 @@ static void carrier_predict(Ctx& x, int stage) {
       ep.X0 = x.F6 + x0I[i] * S;
       ep.X1 = x.F6 + x1I[i] * S;
       ep.s = 1.0;
-      gemm(x, x.D1p, x.F6 + inI[i] * S, S, x.ADV + i * S, S, 1, ep);
+      gemm(x, x.opD1, x.F6 + inI[i] * S, S, x.ADV + i * S, S, 1, ep);
     }
-    grad_u();
+    // only the wall rows of du_i/dz are read in this form
+    wall_dz(x.U, x.DU, S, x.M, x.nz, x.d1r0, x.d1rn, x.s);
   } else {
     grad_u();
     bwd<T>(x, x.DU, dup, 9 * x.nz);
@@ -471,7 +459,7 @@ static void carrier_predict(Ctx& x, int stage) {
     ep.dy2 = x.dy2;
     ep.a = redtc3;
     ep.c2 = c2;
-    gemm(x, x.D2p, x.U, S, x.RHS, S, 3, ep);
+    gemm(x, x.opD2, x.U, S, x.RHS, S, 3, ep);
   }
   // FlatCarrierBoundary::Apply (boundary_carrier_flat.cc:185-246) + top mean values
   {
@@ -506,8 +494,8 @@ static void carrier_predict(Ctx& x, int stage) {
     ep.k2 = x.k2;
     ep.sigma = x.sig_u[stage];
     ep.null_mode = std::fabs(ep.sigma) < kSmall;
-    gemm(x, x.Einvf[i], x.RHS + i * S, S, x.TMP + i * S, S, 1, ep);
-    gemm(x, x.Ef[i], x.TMP + i * S, S, x.SU + i * S, S, 1, EpiParams());
+    gemm(x, x.opEinv[i], x.RHS + i * S, S, x.TMP + i * S, S, 1, ep);
+    gemm(x, x.opE[i], x.TMP + i * S, S, x.SU + i * S, S, 1, EpiParams());
   }
 }
 
@@ -526,7 +514,7 @@ static void carrier_correct(Ctx& x, int stage) {
     ep.X0 = x.SU;
     ep.X1 = x.SU + S;
     ep.s = 0.5 / dt / c3;
-    gemm(x, x.D1p, x.SU + 2 * S, S, x.TMP, S, 1, ep);
+    gemm(x, x.opD1, x.SU + 2 * S, S, x.TMP, S, 1, ep);
   }
   {  // Helmholtz, correction branch (phase_carrier_flat.cc:933-987)
     EpiParams ep;
@@ -535,8 +523,8 @@ static void carrier_correct(Ctx& x, int stage) {
     ep.k2 = x.k2;
     ep.sigma = 0.0;
     ep.null_mode = 1;
-    gemm(x, x.Einvf[3], x.TMP, S, x.TMP + S, S, 1, ep);
-    gemm(x, x.Ef[3], x.TMP + S, S, x.PR, S, 1, EpiParams());
+    gemm(x, x.opEinv[3], x.TMP, S, x.TMP + S, S, 1, ep);
+    gemm(x, x.opE[3], x.TMP + S, S, x.PR, S, 1, EpiParams());
   }
   {  // grad p (phase_carrier_flat.cc:597)
     EpiParams ep;
@@ -546,7 +534,7 @@ static void carrier_correct(Ctx& x, int stage) {
     ep.X0 = x.PR;
     ep.aux0 = x.DP;
     ep.aux1 = x.DP + S;
-    gemm(x, x.D1p, x.PR, S, x.DP + 2 * S, S, 1, ep);
+    gemm(x, x.opD1, x.PR, S, x.DP + 2 * S, S, 1, ep);
   }
   if (stage == 2) x.olddt = dt;   // boundary_carrier_flat.cc:140-142
   boundary_update(x.hist, x.DP, S, x.M, x.nz, x.opentop ? 1 : 0, x.kx, x.ky, x.d1r0, x.d1rn, x.s);
@@ -592,7 +580,7 @@ static void scalar_correct(Ctx& x, int stage) {
     ep.X0 = x.F6;
     ep.X1 = x.F6 + S;
     ep.s = 1.0;
-    gemm(x, x.D1p, x.F6 + 2 * S, S, x.ADVPHI, S, 1, ep);
+    gemm(x, x.opD1, x.F6 + 2 * S, S, x.ADVPHI, S, 1, ep);
   } else {
     EpiParams ep;
     ep.mode = EPI_GRAD;
@@ -601,7 +589,7 @@ static void scalar_correct(Ctx& x, int stage) {
     ep.X0 = x.PHI;
     ep.aux0 = x.TMP;
     ep.aux1 = x.TMP + S;
-    gemm(x, x.D1p, x.PHI, S, x.TMP + 2 * S, S, 1, ep);
+    gemm(x, x.opD1, x.PHI, S, x.TMP + 2 * S, S, 1, ep);
     bwd<T>(x, x.TMP, dup, 3 * x.nz);
     adv_products<T>(unl, dup, prd, P, 1, s0, s1, s2, x.s);
     fwd<T>(x, prd, x.ADVPHI, x.nz);
@@ -617,7 +605,7 @@ static void scalar_correct(Ctx& x, int stage) {
     ep.dy2 = x.dy2;
     ep.a = redtc3;
     ep.c2 = c2;
-    gemm(x, x.D2p, x.PHI, S, x.RHSPHI, S, 1, ep);
+    gemm(x, x.opD2, x.PHI, S, x.RHSPHI, S, 1, ep);
   }
   zero_rows(x.RHSPHI, x.M, x.nz, x.s);   // FlatScalarBoundary::Apply
   if (c.scalar_bc == 1) {                 // erosion / deposition row (phase_scalar_flat.cc:340-384)
@@ -633,8 +621,8 @@ static void scalar_correct(Ctx& x, int stage) {
     ep.k2 = x.k2;
     ep.sigma = x.sig_s[stage];
     ep.null_mode = std::fabs(ep.sigma) < kSmall;
-    gemm(x, x.Einvf[4], x.RHSPHI, S, x.TMP, S, 1, ep);
-    gemm(x, x.Ef[4], x.TMP, S, x.PHI, S, 1, EpiParams());
+    gemm(x, x.opEinv[4], x.RHSPHI, S, x.TMP, S, 1, ep);
+    gemm(x, x.opE[4], x.TMP, S, x.PHI, S, 1, EpiParams());
   }
   // Bartnicki positivity filter (phase_scalar_flat.cc:419-478)
   bwd<T>(x, x.PHI, phip, x.nz);
@@ -687,7 +675,7 @@ static void upload_state(Ctx& x, const double* uvw, const double* p, const doubl
   ep.X0 = x.PR;
   ep.aux0 = x.DP;
   ep.aux1 = x.DP + S;
-  gemm(x, x.D1p, x.PR, S, x.DP + 2 * S, S, 1, ep);
+  gemm(x, x.opD1, x.PR, S, x.DP + 2 * S, S, 1, ep);
   TG_CUDA(cudaMemsetAsync(x.H, 0, 3 * S * sizeof(double2), x.s));
   TG_CUDA(cudaMemsetAsync(x.hist, 0, 24 * (size_t)x.M * sizeof(double2), x.s));
   TG_CUDA(cudaMemsetAsync(x.DU, 0, 9 * S * sizeof(double2), x.s));
@@ -1122,8 +1110,8 @@ tg_status tg_multiply(tg_ctx* ctx, const double* A_host, const double* in, doubl
   TG_TRY({
     TG_CUDA(cudaStreamSynchronize(x.s));
     std::vector<double> A(A_host, A_host + (size_t)x.nz * x.nz);
-    upload_padded(x, x.Atmp, A);
-    gemm(x, x.Atmp, reinterpret_cast<const double2*>(in), x.S, reinterpret_cast<double2*>(out), x.S, dim,
+    zop_build(x.opTmp, A, x.nz, true, allocator(x));
+    gemm(x, x.opTmp, reinterpret_cast<const double2*>(in), x.S, reinterpret_cast<double2*>(out), x.S, dim,
          EpiParams());
   });
 }
@@ -1142,8 +1130,8 @@ tg_status tg_helmholtz(tg_ctx* ctx, int which, int stage, const double* rhs, dou
     ep.k2 = x.k2;
     ep.sigma = which < 3 ? x.sig_u[stage] : (which == 3 ? 0.0 : x.sig_s[stage]);
     ep.null_mode = std::fabs(ep.sigma) < kSmall;
-    gemm(x, x.Einvf[which], reinterpret_cast<const double2*>(rhs), x.S, x.TMP, x.S, 1, ep);
-    gemm(x, x.Ef[which], x.TMP, x.S, reinterpret_cast<double2*>(out), x.S, 1, EpiParams());
+    gemm(x, x.opEinv[which], reinterpret_cast<const double2*>(rhs), x.S, x.TMP, x.S, 1, ep);
+    gemm(x, x.opE[which], x.TMP, x.S, reinterpret_cast<double2*>(out), x.S, 1, EpiParams());
   });
 }
 

@@ -266,6 +266,36 @@ void boundary_update(double2* hist, const double2* dp, size_t S, int M, int nz, 
   TG_LAUNCH_CHECK("k_boundary_update");
 }
 
+// Wall rows of d(u_i)/dz only (rows 0 and N-1 of D1*u_i, i = 0..2): all the
+// divergence-form step reads of the velocity gradient (bottom plane for the
+// erosion flux, phase_scalar_flat.cc:349-353; mean-mode wall values for the
+// features, phase_carrier_flat.cc:687-692).
+__global__ void k_wall_dz(const double2* __restrict__ U, double2* __restrict__ DU, size_t S, int M, int nz,
+                          const double* __restrict__ d1r0, const double* __restrict__ d1rn) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < 3 * M; t += gridDim.x * blockDim.x) {
+    const int c = t / M, m = t - c * M;
+    const double2* u = U + (size_t)c * S + m;
+    double s0x = 0, s0y = 0, snx = 0, sny = 0;
+    for (int k = 0; k < nz; ++k) {
+      double2 v = u[(size_t)k * M];
+      s0x += d1r0[k] * v.x;
+      s0y += d1r0[k] * v.y;
+      snx += d1rn[k] * v.x;
+      sny += d1rn[k] * v.y;
+    }
+    double2* dz = DU + (size_t)(3 * c + 2) * S + m;
+    dz[0] = make_double2(s0x, s0y);
+    dz[(size_t)(nz - 1) * M] = make_double2(snx, sny);
+  }
+}
+void wall_dz(const double2* U, double2* DU, size_t S, int M, int nz, const double* d1r0, const double* d1rn,
+             cudaStream_t s) {
+  prof_begin(s, PC_ELEM, 3.0 * 16.0 * (double)S, 0);
+  k_wall_dz<<<nblk(3 * (size_t)M), kT, 0, s>>>(U, DU, S, M, nz, d1r0, d1rn);
+  prof_end(s);
+  TG_LAUNCH_CHECK("k_wall_dz");
+}
+
 // projection u = u* - 2 dt c3 grad p, mean w := 0 (phase_carrier_flat.cc:609-620)
 __global__ void k_project(double2* __restrict__ U, const double2* __restrict__ SU, const double2* __restrict__ DP,
                           size_t S, int M, double coef) {

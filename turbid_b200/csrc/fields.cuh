@@ -22,6 +22,8 @@ void boundary_apply(double2* rhs, const double2* hist, size_t S, int M, int nz, 
                     double tu, double tv, double tw, cudaStream_t s);
 void boundary_update(double2* hist, const double2* dp, size_t S, int M, int nz, int opentop, const double* kx,
                      const double* ky, const double* d1r0, const double* d1rn, cudaStream_t s);
+void wall_dz(const double2* U, double2* DU, size_t S, int M, int nz, const double* d1r0, const double* d1rn,
+             cudaStream_t s);
 void project(double2* U, const double2* SU, const double2* DP, size_t S, int M, double coef, cudaStream_t s);
 void zero_rows(double2* f, int M, int nz, cudaStream_t s);
 template <typename T>

@@ -5,24 +5,36 @@
 // In the z-slab layout a spectral component is a row-major (Nz x 2M) real
 // matrix (row = z plane, column = re/im of mode m), so applying a real Nz x Nz
 // operator along z is the plain GEMM  out = A * in  with a K dimension of Nz.
-// FP64 tiles run on the FP64 tensor-core path (mma.sync m8n8k4 f64), operands
-// staged through shared memory with cp.async double buffering.  Each
-// accumulator pair of a thread is one complex number (re, im) of mode m, so
-// the epilogues that follow the reference's Armadillo expressions (reciprocal
-// scaling, divergence, Laplacian + right-hand side, gradient) run per element
-// on the accumulators before the single store.
+// Tiles run on the FP64 tensor-core path (mma.sync m8n8k4 f64), operands
+// staged through shared memory with double buffering.  Each accumulator pair
+// of a thread is one complex number (re, im) of mode m, so the epilogues that
+// follow the reference's Armadillo expressions (reciprocal scaling,
+// divergence, Laplacian + right-hand side, gradient) run per element on the
+// accumulators before the single store.
+//
+// Two kernels:
+//   dense: CTA = MT*8 output rows x 128 reals; 8 warps, each all MT m-tiles x
+//          2 n-tiles; MT chosen per Nz so the row tiles cover Nz with little
+//          padding (257 rows = 3 tiles of 88).
+//   sym:   operators with A[n-1-i][n-1-j] = s*A[i][j] (s = +1 for D2, -1 for
+//          D1 on the Chebyshev-Gauss-Lobatto grid).  With h = (n-1)/2 and the
+//          folded input  xe[k] = x[k] + x[n-1-k] (k < h), xe[h] = x[h],
+//          xo[k] = x[k] - x[n-1-k]  the product is P = Ae*xe, Q = Ao*xo with
+//          Ae[i][j] = (A[i][j] + A[i][n-1-j])/2, Ao[i][j] = (A[i][j] - A[i][n-1-j])/2
+//          (j < h), Ae[i][h] = A[i][h], and  y[i] = P + Q, y[n-1-i] = s (P - Q)
+//          for i <= h: half the flops of the dense product.  CTA = MT*8 folded
+//          rows x 64 reals; each warp holds P and Q of one n-tile.
+#include <algorithm>
+#include <cmath>
+
 #include "tg_common.cuh"
 
 namespace tg {
 
 namespace {
-constexpr int BM = 64;    // rows (output z) per CTA
-constexpr int BN = 128;   // columns (reals = 64 complex modes) per CTA
-constexpr int BK = 16;    // K (input z) per pipeline stage
-constexpr int AST = BK + 4;   // smem row stride of A (doubles): conflict-free fragments
-constexpr int BST = BN + 4;   // smem row stride of B
+constexpr int BK = 16;          // K per pipeline stage
+constexpr int AST = BK + 4;     // smem row stride of A tiles (doubles): conflict-free fragments
 constexpr int kThreads = 256;
-constexpr size_t kSmem = 2 * (BM * AST + BK * BST) * sizeof(double);
 
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool valid) {
   unsigned s = (unsigned)__cvta_generic_to_shared(smem);
@@ -81,57 +93,65 @@ __device__ __forceinline__ double2 epilogue(const EpiParams& ep, int b, int r, i
   }
 }
 
-// A: padded (rowsPad x lda) zero-filled beyond (rows x K); lda % BK == 0.
-__global__ void __launch_bounds__(kThreads) zgemm64_kernel(const double* __restrict__ A, int lda, int rows, int K,
-                                                           const double* __restrict__ Bm, long long in_stride,
-                                                           double* __restrict__ Cm, long long out_stride, int M,
-                                                           EpiParams ep) {
+struct GemmArgs {
+  const double* A;    // dense: A; sym: Ae      (rows padded x lda, zero padded)
+  const double* Ao;   // sym: Ao
+  int lda;
+  int rows;           // dense: output rows; sym: folded rows h+1
+  int K;              // dense: Nz; sym: h+1
+  int nz;             // physical rows
+  int sgn;            // sym: +1 / -1
+  const double* B;
+  long long in_stride;   // complex elements between batch components
+  double* C;
+  long long out_stride;
+  int M;
+  EpiParams ep;
+};
+
+// ---------------------------------------------------------------------------
+// dense: out rows [r0, r0 + 8*MT), columns [j0, j0 + 128) reals
+// ---------------------------------------------------------------------------
+template <int MT>
+__global__ void __launch_bounds__(kThreads) zgemm_dense_kernel(GemmArgs g) {
+  constexpr int BM = 8 * MT, BN = 128, BST = BN + 4;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  double* As = reinterpret_cast<double*>(smem_raw);       // [2][BM][AST]
-  double* Bs = As + 2 * BM * AST;                           // [2][BK][BST]
-  const int ncol = 2 * M;
+  double* As = reinterpret_cast<double*>(smem_raw);   // [2][BM][AST]
+  double* Bs = As + 2 * BM * AST;                      // [2][BK][BST]
+  const int ncol = 2 * g.M;
   const int r0 = blockIdx.x * BM;
   const int j0 = blockIdx.y * BN;
   const int b = blockIdx.z;
-  const double* Bb = Bm + (size_t)b * in_stride * 2;
-  const int tid = threadIdx.x;
-  const int lane = tid & 31, warp = tid >> 5;
-  const int wr = warp >> 2, wc = warp & 3;
-  const int nkt = (K + BK - 1) / BK;
+  const double* Bb = g.B + (size_t)b * g.in_stride * 2;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int nkt = (g.K + BK - 1) / BK;
+  int mt_valid = (g.rows - r0 + 7) / 8;
+  mt_valid = mt_valid > MT ? MT : mt_valid;
 
   auto load_tile = [&](int kt, int buf) {
     const int k0 = kt * BK;
-    // A: BM x BK doubles = 512 double2 chunks, 2 per thread
     double* as = As + buf * BM * AST;
-#pragma unroll
-    for (int i = 0; i < 2; ++i) {
-      int c = tid + i * kThreads;        // 0..511
-      int row = c >> 3, kk = (c & 7) * 2;
-      cp_async16(as + row * AST + kk, A + (size_t)(r0 + row) * lda + k0 + kk, true);
+    for (int c = tid; c < BM * (BK / 2); c += kThreads) {
+      int row = c / (BK / 2), kk = (c % (BK / 2)) * 2;
+      cp_async16(as + row * AST + kk, g.A + (size_t)(r0 + row) * g.lda + k0 + kk, true);
     }
-    // B: BK x BN doubles = 1024 double2 chunks, 4 per thread
     double* bs = Bs + buf * BK * BST;
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      int c = tid + i * kThreads;        // 0..1023
-      int kr = c >> 6, jj = (c & 63) * 2;
+    for (int i = 0; i < (BK * BN / 2) / kThreads; ++i) {
+      int c = tid + i * kThreads;
+      int kr = c / (BN / 2), jj = (c % (BN / 2)) * 2;
       int k = k0 + kr, j = j0 + jj;
-      bool ok = (k < K) && (j < ncol);
+      bool ok = (k < g.K) && (j < ncol);
       const double* src = ok ? (Bb + (size_t)k * ncol + j) : Bb;
       cp_async16(bs + kr * BST + jj, src, ok);
     }
   };
 
-  double acc[4][4][2];
+  double acc[MT][2][2];
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
+  for (int i = 0; i < MT; ++i)
 #pragma unroll
-    for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
-
-  // rows of this warp that exist (ragged last row tile): skip empty m-tiles
-  const int wrow0 = r0 + wr * 32;
-  int mtiles = (rows - wrow0 + 7) / 8;
-  mtiles = mtiles < 0 ? 0 : (mtiles > 4 ? 4 : mtiles);
+    for (int j = 0; j < 2; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
 
   load_tile(0, 0);
   cp_async_commit();
@@ -147,19 +167,19 @@ __global__ void __launch_bounds__(kThreads) zgemm64_kernel(const double* __restr
     __syncthreads();
     const double* as = As + buf * BM * AST;
     const double* bs = Bs + buf * BK * BST;
-    if (mtiles > 0) {
+    const int ksteps = min(BK / 4, (g.K - kt * BK + 3) / 4);   // skip the zero K tail
 #pragma unroll
-      for (int ks = 0; ks < BK / 4; ++ks) {
-        double af[4], bf[4];
+    for (int ks = 0; ks < BK / 4; ++ks) {
+      if (ks < ksteps) {
+        double bf[2];
 #pragma unroll
-        for (int mt = 0; mt < 4; ++mt) af[mt] = as[(wr * 32 + mt * 8 + (lane >> 2)) * AST + ks * 4 + (lane & 3)];
+        for (int nt = 0; nt < 2; ++nt) bf[nt] = bs[(ks * 4 + (lane & 3)) * BST + warp * 16 + nt * 8 + (lane >> 2)];
 #pragma unroll
-        for (int nt = 0; nt < 4; ++nt) bf[nt] = bs[(ks * 4 + (lane & 3)) * BST + wc * 32 + nt * 8 + (lane >> 2)];
-#pragma unroll
-        for (int mt = 0; mt < 4; ++mt) {
-          if (mt < mtiles) {
-#pragma unroll
-            for (int nt = 0; nt < 4; ++nt) dmma(acc[mt][nt][0], acc[mt][nt][1], af[mt], bf[nt]);
+        for (int mt = 0; mt < MT; ++mt) {
+          if (mt < mt_valid) {
+            double af = as[(mt * 8 + (lane >> 2)) * AST + ks * 4 + (lane & 3)];
+            dmma(acc[mt][0][0], acc[mt][0][1], af, bf[0]);
+            dmma(acc[mt][1][0], acc[mt][1][1], af, bf[1]);
           }
         }
       }
@@ -167,38 +187,275 @@ __global__ void __launch_bounds__(kThreads) zgemm64_kernel(const double* __restr
     __syncthreads();
   }
 
-  // epilogue: thread holds (re, im) of one complex mode per (mt, nt)
-  double2* Cb = reinterpret_cast<double2*>(Cm) + (size_t)b * out_stride;
+  double2* Cb = reinterpret_cast<double2*>(g.C) + (size_t)b * g.out_stride;
 #pragma unroll
-  for (int mt = 0; mt < 4; ++mt) {
-    const int r = wrow0 + mt * 8 + (lane >> 2);
-    if (r >= rows) continue;
+  for (int mt = 0; mt < MT; ++mt) {
+    const int r = r0 + mt * 8 + (lane >> 2);
+    if (r >= g.rows) continue;
 #pragma unroll
-    for (int nt = 0; nt < 4; ++nt) {
-      const int m = (j0 + wc * 32 + nt * 8) / 2 + (lane & 3);
-      if (m >= M) continue;
-      double2 v = epilogue(ep, b, r, m, make_double2(acc[mt][nt][0], acc[mt][nt][1]));
-      Cb[(size_t)r * M + m] = v;
+    for (int nt = 0; nt < 2; ++nt) {
+      const int m = (j0 + warp * 16 + nt * 8) / 2 + (lane & 3);
+      if (m >= g.M) continue;
+      Cb[(size_t)r * g.M + m] = epilogue(g.ep, b, r, m, make_double2(acc[mt][nt][0], acc[mt][nt][1]));
     }
   }
 }
+
+// ---------------------------------------------------------------------------
+// sym: folded rows [r0, r0 + 8*MT) of P and Q, columns [j0, j0 + 64) reals
+// ---------------------------------------------------------------------------
+template <int MT>
+__global__ void __launch_bounds__(kThreads) zgemm_sym_kernel(GemmArgs g) {
+  constexpr int BM = 8 * MT, BN = 64, BST = BN + 4;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double* Ae = reinterpret_cast<double*>(smem_raw);   // [2][BM][AST]
+  double* Ao = Ae + 2 * BM * AST;                      // [2][BM][AST]
+  double* Be = Ao + 2 * BM * AST;                      // [2][BK][BST]
+  double* Bo = Be + 2 * BK * BST;                      // [2][BK][BST]
+  const int ncol = 2 * g.M;
+  const int n = g.nz, h = (g.nz - 1) / 2;
+  const int r0 = blockIdx.x * BM;
+  const int j0 = blockIdx.y * BN;
+  const int b = blockIdx.z;
+  const double* Bb = g.B + (size_t)b * g.in_stride * 2;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int nkt = (g.K + BK - 1) / BK;
+  int mt_valid = (g.rows - r0 + 7) / 8;
+  mt_valid = mt_valid > MT ? MT : mt_valid;
+
+  // B tile: BK folded rows x 64 reals = 512 double2 per parity, 2 per thread
+  constexpr int BPT = (BK * BN / 2) / kThreads;
+  double2 lo[BPT], hi[BPT];
+  auto fetch_b = [&](int kt) {
+    const int k0 = kt * BK;
+#pragma unroll
+    for (int i = 0; i < BPT; ++i) {
+      int c = tid + i * kThreads;
+      int kr = c / (BN / 2), jj = (c % (BN / 2)) * 2;
+      int k = k0 + kr, j = j0 + jj;
+      lo[i] = make_double2(0.0, 0.0);
+      hi[i] = make_double2(0.0, 0.0);
+      if (k <= h && j < ncol) {
+        lo[i] = *reinterpret_cast<const double2*>(Bb + (size_t)k * ncol + j);
+        if (k < h) hi[i] = *reinterpret_cast<const double2*>(Bb + (size_t)(n - 1 - k) * ncol + j);
+      }
+    }
+  };
+  auto store_b = [&](int buf) {
+    double* be = Be + buf * BK * BST;
+    double* bo = Bo + buf * BK * BST;
+#pragma unroll
+    for (int i = 0; i < BPT; ++i) {
+      int c = tid + i * kThreads;
+      int kr = c / (BN / 2), jj = (c % (BN / 2)) * 2;
+      *reinterpret_cast<double2*>(be + kr * BST + jj) = make_double2(lo[i].x + hi[i].x, lo[i].y + hi[i].y);
+      *reinterpret_cast<double2*>(bo + kr * BST + jj) = make_double2(lo[i].x - hi[i].x, lo[i].y - hi[i].y);
+    }
+  };
+  auto load_a = [&](int kt, int buf) {
+    const int k0 = kt * BK;
+    double* ae = Ae + buf * BM * AST;
+    double* ao = Ao + buf * BM * AST;
+    for (int c = tid; c < BM * (BK / 2); c += kThreads) {
+      int row = c / (BK / 2), kk = (c % (BK / 2)) * 2;
+      cp_async16(ae + row * AST + kk, g.A + (size_t)(r0 + row) * g.lda + k0 + kk, true);
+      cp_async16(ao + row * AST + kk, g.Ao + (size_t)(r0 + row) * g.lda + k0 + kk, true);
+    }
+  };
+
+  double accE[MT][2], accO[MT][2];
+#pragma unroll
+  for (int i = 0; i < MT; ++i) accE[i][0] = accE[i][1] = accO[i][0] = accO[i][1] = 0.0;
+
+  load_a(0, 0);
+  cp_async_commit();
+  fetch_b(0);
+  store_b(0);
+  for (int kt = 0; kt < nkt; ++kt) {
+    const int buf = kt & 1;
+    const bool more = kt + 1 < nkt;
+    if (more) {
+      load_a(kt + 1, buf ^ 1);
+      cp_async_commit();
+      fetch_b(kt + 1);   // global loads in flight during this tile's math
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+    const double* ae = Ae + buf * BM * AST;
+    const double* ao = Ao + buf * BM * AST;
+    const double* be = Be + buf * BK * BST;
+    const double* bo = Bo + buf * BK * BST;
+    const int ksteps = min(BK / 4, (g.K - kt * BK + 3) / 4);
+#pragma unroll
+    for (int ks = 0; ks < BK / 4; ++ks) {
+      if (ks < ksteps) {
+        const int bi = (ks * 4 + (lane & 3)) * BST + warp * 8 + (lane >> 2);
+        const double bfe = be[bi], bfo = bo[bi];
+#pragma unroll
+        for (int mt = 0; mt < MT; ++mt) {
+          if (mt < mt_valid) {
+            const int ai = (mt * 8 + (lane >> 2)) * AST + ks * 4 + (lane & 3);
+            dmma(accE[mt][0], accE[mt][1], ae[ai], bfe);
+            dmma(accO[mt][0], accO[mt][1], ao[ai], bfo);
+          }
+        }
+      }
+    }
+    if (more) store_b(buf ^ 1);   // its last readers finished before the barrier above
+    __syncthreads();
+  }
+
+  double2* Cb = reinterpret_cast<double2*>(g.C) + (size_t)b * g.out_stride;
+  const double s = (double)g.sgn;
+#pragma unroll
+  for (int mt = 0; mt < MT; ++mt) {
+    const int i = r0 + mt * 8 + (lane >> 2);
+    if (i > h) continue;
+    const int m = (j0 + warp * 8) / 2 + (lane & 3);
+    if (m >= g.M) continue;
+    const double pe = accE[mt][0], pi = accE[mt][1], qe = accO[mt][0], qi = accO[mt][1];
+    Cb[(size_t)i * g.M + m] = epilogue(g.ep, b, i, m, make_double2(pe + qe, pi + qi));
+    if (i < h) {
+      const int j = n - 1 - i;
+      Cb[(size_t)j * g.M + m] = epilogue(g.ep, b, j, m, make_double2(s * (pe - qe), s * (pi - qi)));
+    }
+  }
+}
+
+template <int MT>
+size_t dense_smem() {
+  return 2 * (8 * MT * AST + BK * (128 + 4)) * sizeof(double);
+}
+template <int MT>
+size_t sym_smem() {
+  return 2 * (2 * 8 * MT * AST + 2 * BK * (64 + 4)) * sizeof(double);
+}
+
+#define TG_MT_LIST(X) X(1) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12) X(13) X(14) X(15) X(16)
+
 }  // namespace
 
 void zgemm_init() {
-  TG_CUDA(cudaFuncSetAttribute(zgemm64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem));
+#define TG_SET(MT)                                                                                           \
+  TG_CUDA(cudaFuncSetAttribute(zgemm_dense_kernel<MT>, cudaFuncAttributeMaxDynamicSharedMemorySize,         \
+                               (int)dense_smem<MT>()));                                                      \
+  TG_CUDA(cudaFuncSetAttribute(zgemm_sym_kernel<MT>, cudaFuncAttributeMaxDynamicSharedMemorySize,           \
+                               (int)sym_smem<MT>()));
+  TG_MT_LIST(TG_SET)
+#undef TG_SET
 }
 
-void zgemm(const double* A, int lda, int rows, int K, const double2* in, long long in_stride, double2* out,
-           long long out_stride, int M, int batch, const EpiParams& ep, cudaStream_t s) {
-  if (lda % BK != 0) throw Error{TG_ERR_ARG, "zgemm > lda must be a multiple of 16"};
-  dim3 grid((rows + BM - 1) / BM, (2 * M + BN - 1) / BN, batch);
-  const double fl = 4.0 * rows * K * (double)M * batch;
-  const double by = (double)batch * 16.0 * M * (K + rows) + 8.0 * rows * K;
+// m-tiles per CTA for `rows` rows: as few row tiles as possible with at most 16
+// m-tiles each, then the tiles as even as possible
+void row_tiling(int rows, int& mt, int& tiles) {
+  const int need = (rows + 7) / 8;
+  tiles = (need + 15) / 16;
+  mt = (need + tiles - 1) / tiles;
+}
+
+void zgemm(const ZOperator& op, const double2* in, long long in_stride, double2* out, long long out_stride, int M,
+           int batch, const EpiParams& ep, cudaStream_t s) {
+  GemmArgs g;
+  g.lda = op.lda;
+  g.nz = op.n;
+  g.B = reinterpret_cast<const double*>(in);
+  g.in_stride = in_stride;
+  g.C = reinterpret_cast<double*>(out);
+  g.out_stride = out_stride;
+  g.M = M;
+  g.ep = ep;
+  // flops executed (the folded product does two (h+1)^2 halves), bytes in + out + operator
+  const double fl = (op.sym ? 2.0 * 4.0 * op.rows * op.rows : 4.0 * op.n * op.n) * (double)M * batch;
+  const double by = (double)batch * 16.0 * M * 2 * op.n + 8.0 * op.n * op.n;
   prof_begin(s, PC_GEMM, by, fl);
-  zgemm64_kernel<<<grid, kThreads, kSmem, s>>>(A, lda, rows, K, reinterpret_cast<const double*>(in), in_stride,
-                                               reinterpret_cast<double*>(out), out_stride, M, ep);
+  if (op.sym) {
+    g.A = op.Ae;
+    g.Ao = op.Ao;
+    g.rows = op.rows;
+    g.K = op.rows;
+    g.sgn = op.sgn;
+    dim3 grid(op.tiles, (2 * M + 63) / 64, batch);
+#define TG_CASE(MT) \
+  case MT: zgemm_sym_kernel<MT><<<grid, kThreads, sym_smem<MT>(), s>>>(g); break;
+    switch (op.mt) { TG_MT_LIST(TG_CASE) default: throw Error{TG_ERR_ARG, "zgemm > bad tiling"}; }
+#undef TG_CASE
+  } else {
+    g.A = op.A;
+    g.Ao = nullptr;
+    g.rows = op.n;
+    g.K = op.n;
+    g.sgn = 1;
+    dim3 grid(op.tiles, (2 * M + 127) / 128, batch);
+#define TG_CASE(MT) \
+  case MT: zgemm_dense_kernel<MT><<<grid, kThreads, dense_smem<MT>(), s>>>(g); break;
+    switch (op.mt) { TG_MT_LIST(TG_CASE) default: throw Error{TG_ERR_ARG, "zgemm > bad tiling"}; }
+#undef TG_CASE
+  }
   prof_end(s);
-  TG_LAUNCH_CHECK("zgemm64_kernel");
+  TG_LAUNCH_CHECK("zgemm kernel");
+}
+
+// Upload an nz x nz operator: the dense copy always; the folded halves when
+// the operator is centro-symmetric (sgn = +1) or centro-antisymmetric
+// (sgn = -1) to within 1e-12 of its largest entry and allow_sym is set.
+void zop_build(ZOperator& op, const std::vector<double>& A, int n, bool allow_sym,
+               const std::function<double*(size_t)>& alloc) {
+  op.n = n;
+  op.lda = (n + 15) / 16 * 16;
+  row_tiling(n, op.mt_dense, op.tiles_dense);
+  const int h = (n - 1) / 2;
+  const int hr = h + 1;   // folded rows
+  int mts, ts;
+  row_tiling(hr, mts, ts);
+  const int rowsAlloc = std::max(op.tiles_dense * op.mt_dense * 8, ts * mts * 8);
+  if (op.rowsPad == 0) op.rowsPad = rowsAlloc;
+  if (op.rowsPad < rowsAlloc) throw Error{TG_ERR_ARG, "zop_build > operator buffer too small"};
+  const size_t sz = (size_t)op.rowsPad * op.lda;
+  if (!op.A) op.A = alloc(sz);
+  std::vector<double> pad(sz, 0.0);
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < n; ++j) pad[(size_t)i * op.lda + j] = A[(size_t)i * n + j];
+  TG_CUDA(cudaMemcpy(op.A, pad.data(), sz * sizeof(double), cudaMemcpyHostToDevice));
+  op.sym = false;
+  if (allow_sym && (n & 1) && n >= 5) {
+    double amax = 0.0;
+    for (double v : A) amax = std::max(amax, std::fabs(v));
+    for (int sgn : {+1, -1}) {
+      double dev = 0.0;
+      for (int i = 0; i < n; ++i)
+        for (int j = 0; j < n; ++j)
+          dev = std::max(dev, std::fabs(A[(size_t)(n - 1 - i) * n + (n - 1 - j)] - sgn * A[(size_t)i * n + j]));
+      if (dev <= 1e-12 * amax) {
+        op.sym = true;
+        op.sgn = sgn;
+        break;
+      }
+    }
+  }
+  if (op.sym) {
+    op.rows = hr;
+    op.mt = mts;
+    op.tiles = ts;
+    if (!op.Ae) op.Ae = alloc(sz);
+    if (!op.Ao) op.Ao = alloc(sz);
+    std::vector<double> ae(sz, 0.0), ao(sz, 0.0);
+    for (int i = 0; i < hr; ++i) {
+      for (int j = 0; j < h; ++j) {
+        const double a = A[(size_t)i * n + j], c = A[(size_t)i * n + (n - 1 - j)];
+        ae[(size_t)i * op.lda + j] = (a + c) / 2;
+        ao[(size_t)i * op.lda + j] = (a - c) / 2;
+      }
+      ae[(size_t)i * op.lda + h] = A[(size_t)i * n + h];
+    }
+    TG_CUDA(cudaMemcpy(op.Ae, ae.data(), sz * sizeof(double), cudaMemcpyHostToDevice));
+    TG_CUDA(cudaMemcpy(op.Ao, ao.data(), sz * sizeof(double), cudaMemcpyHostToDevice));
+  } else {
+    op.rows = n;
+    op.mt = op.mt_dense;
+    op.tiles = op.tiles_dense;
+  }
 }
 
 }  // namespace tg

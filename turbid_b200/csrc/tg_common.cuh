@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -135,8 +136,25 @@ struct EpiParams {
   long long sX = 0, sH = 0, sU = 0, sAux = 0;
 };
 
+// A real nz x nz operator resident on the device: the dense copy and, when
+// it is centro-symmetric (sgn +1) or centro-antisymmetric (sgn -1), the two
+// folded halves used by the half-flop kernel.
+struct ZOperator {
+  int n = 0, lda = 0, rowsPad = 0;
+  bool sym = false;
+  int sgn = 1;
+  int rows = 0, mt = 0, tiles = 0;       // launch shape of the kernel used
+  int mt_dense = 0, tiles_dense = 0;
+  double* A = nullptr;
+  double* Ae = nullptr;
+  double* Ao = nullptr;
+};
+
 void zgemm_init();
-void zgemm(const double* A, int lda, int rows, int K, const double2* in, long long in_stride, double2* out,
-           long long out_stride, int M, int batch, const EpiParams& ep, cudaStream_t s);
+void row_tiling(int rows, int& mt, int& tiles);
+void zop_build(ZOperator& op, const std::vector<double>& A, int n, bool allow_sym,
+               const std::function<double*(size_t)>& alloc);
+void zgemm(const ZOperator& op, const double2* in, long long in_stride, double2* out, long long out_stride, int M,
+           int batch, const EpiParams& ep, cudaStream_t s);
 
 }  // namespace tg
