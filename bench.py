@@ -323,10 +323,14 @@ def our_arm(args):
 
     # ---- roofline of the dominant kernel class
     steps_p = max(args.prof_steps, 1)
+    if not any(v["ms"] > 0 for v in prof.values()):
+        prof = {"zgemm": {"ms": 0.0, "bytes": 0.0, "flops": 0.0, "count": 0}}
     dom = max(prof, key=lambda k: prof[k]["ms"])
     d = prof[dom]
     traffic = traffic_summary().get(args.workload, {}).get(prec, {}).get(dom)
-    if dom == "zgemm":
+    if d["ms"] <= 0:
+        roof = None
+    elif dom == "zgemm":
         peak = fp64_gemm_peak(torch)
         achieved = d["flops"] / (d["ms"] * 1e-3) / 1e12
         roof = {"kernel": "zgemm_dense_kernel / zgemm_sym_kernel (FP64 DMMA z-operator GEMM; flops executed)", "bound": "tensor", "achieved": achieved,
