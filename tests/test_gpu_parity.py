@@ -51,7 +51,10 @@ def sediment_cfg(**kw):
 # ----------------------------------------------------------------------------
 # field-container primitives
 # ----------------------------------------------------------------------------
-@pytest.mark.parametrize("shape", [(24, 18, 9), (32, 32, 17), (3, 3, 5), (30, 20, 7)])
+# power-of-two lengths 8..1024 run the in-place radix-16 kernels, the others
+# the mixed-radix kernels; (256, 256, 129) spans several launches (chunks)
+@pytest.mark.parametrize("shape", [(24, 18, 9), (32, 32, 17), (3, 3, 5), (30, 20, 7), (8, 8, 3), (16, 64, 3),
+                                   (1024, 16, 3), (8, 1024, 3), (128, 512, 3), (512, 24, 3), (256, 256, 129)])
 def test_dft_f64_matches_oracle(cuda, shape):
     import torch
     nx, ny, nz = shape
@@ -73,7 +76,8 @@ def test_dft_f64_matches_oracle(cuda, shape):
     gc.close()
 
 
-@pytest.mark.parametrize("shape", [(24, 18, 9), (64, 48, 5)])
+@pytest.mark.parametrize("shape", [(24, 18, 9), (64, 48, 5), (256, 256, 4), (1024, 8, 3), (16, 512, 3),
+                                   (32, 16, 3)])
 def test_dft_f32_matches_oracle(cuda, shape):
     import torch
     nx, ny, nz = shape

@@ -97,6 +97,7 @@ struct Ctx {
   double2 *ADV = nullptr, *DU = nullptr, *F6 = nullptr, *PHI = nullptr, *HPHI = nullptr, *ADVPHI = nullptr;
   double2 *RHSPHI = nullptr, *hist = nullptr, *ero = nullptr, *REF = nullptr;
   void *UNL = nullptr, *DUP = nullptr, *PRD = nullptr, *PHIP = nullptr, *PLN = nullptr, *work = nullptr;
+  int work_planes = 0;  // planes one transform launch pair handles
   double* feat = nullptr;
   unsigned long long* bits = nullptr;
   double* feat_h = nullptr;   // pinned [2][100]
@@ -304,7 +305,10 @@ static Ctx* create(const tg_case& c) {
   x.PRD = x.dalloc<unsigned char>(6 * P * ps);
   x.PHIP = x.dalloc<unsigned char>(P * ps);
   x.PLN = x.dalloc<unsigned char>(3 * (size_t)x.nx * x.ny * ps);
-  x.work = x.dalloc<double2>(9 * (size_t)x.nz * x.nxh * x.ny);
+  // whole-batch transforms (up to nine fields per launch pair): splitting a
+  // batch so its intermediate stays in L2 measured slower (partial last waves)
+  x.work_planes = 9 * x.nz;
+  x.work = x.dalloc<double2>((size_t)x.work_planes * x.nxh * x.ny);
   x.feat = x.dalloc<double>(100);
   x.bits = x.dalloc<unsigned long long>(16);
   TG_CUDA(cudaMallocHost(&x.feat_h, 2 * 100 * sizeof(double)));
@@ -326,16 +330,16 @@ static void gemm(Ctx& x, const ZOperator& A, const double2* in, long long sin, d
 
 template <typename T>
 static void fwd(Ctx& x, const void* phys, double2* spec, int planes) {
-  for (int p0 = 0; p0 < planes; p0 += 9 * x.nz) {
-    int np = std::min(planes - p0, 9 * x.nz);
+  for (int p0 = 0; p0 < planes; p0 += x.work_planes) {
+    int np = std::min(planes - p0, x.work_planes);
     dft_forward<T>(x.td, x.px, x.py, (const T*)phys + (size_t)p0 * x.nx * x.ny, spec + (size_t)p0 * x.M, np,
                    x.work, x.s);
   }
 }
 template <typename T>
 static void bwd(Ctx& x, const double2* spec, void* phys, int planes) {
-  for (int p0 = 0; p0 < planes; p0 += 9 * x.nz) {
-    int np = std::min(planes - p0, 9 * x.nz);
+  for (int p0 = 0; p0 < planes; p0 += x.work_planes) {
+    int np = std::min(planes - p0, x.work_planes);
     dft_backward<T>(x.td, x.px, x.py, spec + (size_t)p0 * x.M, (T*)phys + (size_t)p0 * x.nx * x.ny, np, x.work,
                     x.s);
   }

@@ -407,6 +407,228 @@ __global__ void __launch_bounds__(256) bwd_x_kernel(TransformDims d, PlanArgs pl
 }
 
 // ---------------------------------------------------------------------------
+// Power-of-two lengths: in-place passes on one padded shared buffer.
+//
+// NB transforms of length L per CTA, NB*L/16 threads, every thread holding
+// 16 complex values of a pass in registers (one radix-16 butterfly, or 16/R
+// butterflies of a smaller final radix), so a pass reads all its inputs,
+// synchronises, and writes its outputs in place.  Shared rows are padded with
+// one spare slot per 16 values (index i -> i + i/16) and one more per row, so
+// the stride-16 writes of the first pass and the column accesses of the
+// x <-> y reorder hit distinct banks.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int sp(int i) { return i + (i >> 4); }
+
+template <int L> struct P2 {
+  static constexpr int RS = L + L / 16 + 1;  // padded row stride (complex values)
+};
+
+// complex values per CTA: 4096 in FP32, 2048 in FP64 (about 35 KB of shared memory)
+template <typename T> struct P2Cta {
+  static constexpr int elems = sizeof(T) == 4 ? 4096 : 2048;
+};
+
+template <typename T, int DIR, int L, int NB, int Ns>
+__device__ __forceinline__ void ip_passes(cplx<T>* buf, const cplx<T>* __restrict__ tw) {
+  using C = cplx<T>;
+  if constexpr (Ns < L) {
+    constexpr int rem = L / Ns;
+    constexpr int R = rem >= 16 ? 16 : rem;
+    constexpr int nb = L / R;          // butterflies per transform
+    constexpr int NT = NB * L / 16;    // threads of the CTA
+    constexpr int BPT = 16 / R;        // butterflies per thread
+    constexpr int RS = P2<L>::RS;
+    constexpr int twstep = L / (Ns * R);
+    C v[BPT][R];
+#pragma unroll
+    for (int t = 0; t < BPT; ++t) {
+      const int g = threadIdx.x + t * NT;
+      const int b = g / nb, j = g - b * nb;
+      const C* src = buf + b * RS;
+      const int jm = j % Ns;
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        v[t][r] = src[sp(j + r * nb)];
+        if (Ns > 1 && r > 0) v[t][r] = cmul(v[t][r], tw_get<T, DIR>(tw, jm * r * twstep));
+      }
+      dft_ct<R, DIR>(v[t]);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int t = 0; t < BPT; ++t) {
+      const int g = threadIdx.x + t * NT;
+      const int b = g / nb, j = g - b * nb;
+      const int jm = j % Ns;
+      const int base = (j - jm) * R + jm;
+      C* dst = buf + b * RS;
+#pragma unroll
+      for (int k = 0; k < R; ++k) dst[sp(base + k * Ns)] = v[t][k];
+    }
+    __syncthreads();
+    ip_passes<T, DIR, L, NB, Ns * R>(buf, tw);
+  }
+}
+
+// spectral row iy -> FFT index along y (P3DFFT pruning, reference src/base.cc:228-237)
+__device__ __forceinline__ int y_of(int iy, int ny, int nyc) { return iy < nyc / 2 ? iy : ny - (nyc - iy); }
+
+// forward x pass, L = nx: NB row pairs per CTA, 2 rows packed per complex FFT
+template <typename T, int L, int NB>
+__global__ void __launch_bounds__(NB * L / 16) fx_p2_kernel(TransformDims d, const cplx<T>* __restrict__ tw,
+                                                           const T* __restrict__ phys, cplx<T>* __restrict__ work) {
+  using C = cplx<T>;
+  constexpr int RS = P2<L>::RS, NT = NB * L / 16, rows = 2 * NB;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* buf = reinterpret_cast<C*>(smem_raw);
+  const int plane = blockIdx.y;
+  const int y0 = blockIdx.x * rows;
+  const T* src = phys + (size_t)plane * d.ny * L;
+#pragma unroll 4
+  for (int idx = threadIdx.x; idx < NB * L; idx += NT) {
+    const int p = idx / L, x = idx % L;
+    const int ya = y0 + 2 * p, yb = ya + 1;
+    const T re = ya < d.ny ? src[(size_t)ya * L + x] : T(0);
+    const T im = yb < d.ny ? src[(size_t)yb * L + x] : T(0);
+    buf[p * RS + sp(x)] = mkc<C>(re, im);
+  }
+  __syncthreads();
+  ip_passes<T, -1, L, NB, 1>(buf, tw);
+  C* dst = work + (size_t)plane * d.nxh * d.ny;
+  for (int idx = threadIdx.x; idx < rows * d.nxh; idx += NT) {
+    const int k = idx / rows, q = idx % rows;
+    const int y = y0 + q;
+    if (y >= d.ny) continue;
+    const C* row = buf + (q >> 1) * RS;
+    const C Z = row[sp(k)];
+    const C Zc = cconj(row[sp(k == 0 ? 0 : L - k)]);
+    C X;
+    if ((q & 1) == 0) {
+      X = mkc<C>((Z.x + Zc.x) * T(0.5), (Z.y + Zc.y) * T(0.5));
+    } else {
+      const C D = csub(Z, Zc);
+      X = mkc<C>(D.y * T(0.5), -D.x * T(0.5));
+    }
+    dst[(size_t)k * d.ny + y] = X;
+  }
+}
+
+// forward y pass, L = ny: NB kx columns per CTA, pruned FP64 output scaled by 1/(Nx*Ny)
+template <typename T, int L, int NB>
+__global__ void __launch_bounds__(NB * L / 16) fy_p2_kernel(TransformDims d, const cplx<T>* __restrict__ tw,
+                                                           const cplx<T>* __restrict__ work,
+                                                           double2* __restrict__ spec, double scale) {
+  using C = cplx<T>;
+  constexpr int RS = P2<L>::RS, NT = NB * L / 16;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* buf = reinterpret_cast<C*>(smem_raw);
+  const int plane = blockIdx.y;
+  const int k0 = blockIdx.x * NB;
+  const C* src = work + (size_t)plane * d.nxh * L;
+#pragma unroll 4
+  for (int idx = threadIdx.x; idx < NB * L; idx += NT) {
+    const int c = idx / L, y = idx % L;
+    buf[c * RS + sp(y)] = k0 + c < d.nxh ? src[(size_t)(k0 + c) * L + y] : mkc<C>(0, 0);
+  }
+  __syncthreads();
+  ip_passes<T, -1, L, NB, 1>(buf, tw);
+  double2* dst = spec + (size_t)plane * d.M;
+  const int nyc = d.nyc;
+  for (int idx = threadIdx.x; idx < NB * nyc; idx += NT) {
+    const int c = idx / nyc, iy = idx - c * nyc;
+    const int k = k0 + c;
+    if (k >= d.nxh) break;
+    const C v = buf[c * RS + sp(y_of(iy, L, nyc))];
+    dst[iy + (size_t)nyc * k] = make_double2((double)v.x * scale, (double)v.y * scale);
+  }
+}
+
+// backward y pass: zero-filled pruned modes, unscaled
+template <typename T, int L, int NB>
+__global__ void __launch_bounds__(NB * L / 16) by_p2_kernel(TransformDims d, const cplx<T>* __restrict__ tw,
+                                                           const double2* __restrict__ spec,
+                                                           cplx<T>* __restrict__ work) {
+  using C = cplx<T>;
+  constexpr int RS = P2<L>::RS, NT = NB * L / 16;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* buf = reinterpret_cast<C*>(smem_raw);
+  const int plane = blockIdx.y;
+  const int k0 = blockIdx.x * NB;
+  const int nyc = d.nyc;
+  const int gap = L - nyc;  // FFT indices [nyc/2, L - nyc/2) carry no spectral row
+  for (int idx = threadIdx.x; idx < NB * gap; idx += NT) {
+    const int c = idx / gap, y = nyc / 2 + (idx - c * gap);
+    buf[c * RS + sp(y)] = mkc<C>(0, 0);
+  }
+  const double2* src = spec + (size_t)plane * d.M;
+  for (int idx = threadIdx.x; idx < NB * nyc; idx += NT) {
+    const int c = idx / nyc, iy = idx - c * nyc;
+    const int k = k0 + c;
+    double2 v = k < d.nxh ? src[iy + (size_t)nyc * k] : make_double2(0.0, 0.0);
+    buf[c * RS + sp(y_of(iy, L, nyc))] = mkc<C>((T)v.x, (T)v.y);
+  }
+  __syncthreads();
+  ip_passes<T, +1, L, NB, 1>(buf, tw);
+  C* dst = work + (size_t)plane * d.nxh * L;
+#pragma unroll 4
+  for (int idx = threadIdx.x; idx < NB * L; idx += NT) {
+    const int c = idx / L, y = idx % L;
+    if (k0 + c < d.nxh) dst[(size_t)(k0 + c) * L + y] = buf[c * RS + sp(y)];
+  }
+}
+
+// backward x pass, L = nx: two rows per complex FFT; Im of the kx = 0 coefficient ignored (c2r).
+// Each thread loads one coefficient (coalesced along y); the row pair is combined
+// across adjacent lanes.
+template <typename T, int L, int NB>
+__global__ void __launch_bounds__(NB * L / 16) bx_p2_kernel(TransformDims d, const cplx<T>* __restrict__ tw,
+                                                           const cplx<T>* __restrict__ work, T* __restrict__ phys) {
+  using C = cplx<T>;
+  constexpr int RS = P2<L>::RS, NT = NB * L / 16, rows = 2 * NB;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* buf = reinterpret_cast<C*>(smem_raw);
+  const int plane = blockIdx.y;
+  const int y0 = blockIdx.x * rows;
+  const int nxh = d.nxh;
+  const int gap = L - 2 * nxh + 1;  // FFT indices [nxh, L - nxh] are zero
+  for (int idx = threadIdx.x; idx < NB * gap; idx += NT) {
+    const int p = idx / gap, x = nxh + (idx - p * gap);
+    buf[p * RS + sp(x)] = mkc<C>(0, 0);
+  }
+  const C* src = work + (size_t)plane * nxh * d.ny;
+  const int total = rows * nxh;  // even; the pair (2p, 2p+1) sits in adjacent lanes
+  for (int base = 0; base < total; base += NT) {
+    const int idx = base + threadIdx.x;
+    const bool ok = idx < total;
+    const int k = idx / rows, q = idx % rows;
+    const int y = y0 + q;
+    C h = (ok && y < d.ny) ? src[(size_t)k * d.ny + y] : mkc<C>(0, 0);
+    if (k == 0) h.y = T(0);
+    C o;
+    o.x = __shfl_xor_sync(0xffffffffu, h.x, 1);
+    o.y = __shfl_xor_sync(0xffffffffu, h.y, 1);
+    if (ok) {
+      C* row = buf + (q >> 1) * RS;
+      if ((q & 1) == 0) {  // Z[k] = X1[k] + i X2[k], h1 = h, h2 = o
+        row[sp(k)] = mkc<C>(h.x - o.y, h.y + o.x);
+      } else if (k > 0) {  // Z[L-k] = conj(X1[k]) + i conj(X2[k]), h1 = o, h2 = h
+        row[sp(L - k)] = mkc<C>(o.x + h.y, -o.y + h.x);
+      }
+    }
+  }
+  __syncthreads();
+  ip_passes<T, +1, L, NB, 1>(buf, tw);
+  T* dst = phys + (size_t)plane * d.ny * L;
+#pragma unroll 4
+  for (int idx = threadIdx.x; idx < NB * L; idx += NT) {
+    const int p = idx / L, x = idx % L;
+    const int ya = y0 + 2 * p, yb = ya + 1;
+    const C z = buf[p * RS + sp(x)];
+    if (ya < d.ny) dst[(size_t)ya * L + x] = z.x;
+    if (yb < d.ny) dst[(size_t)yb * L + x] = z.y;
+  }
+}
+
+// ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
 static const size_t kFftSmemBudget = 64 * 1024;
@@ -460,35 +682,72 @@ void fft_init() {
   set_smem_all<float, 0>();
 }
 
+static bool p2_length(int L) { return L >= 8 && L <= 1024 && (L & (L - 1)) == 0; }
+
+#define TG_P2_DISPATCH(L, CALL) \
+  switch (L) {                  \
+    case 8: CALL(8); break;     \
+    case 16: CALL(16); break;   \
+    case 32: CALL(32); break;   \
+    case 64: CALL(64); break;   \
+    case 128: CALL(128); break; \
+    case 256: CALL(256); break; \
+    case 512: CALL(512); break; \
+    case 1024: CALL(1024); break; \
+  }
+
+template <typename T, int L>
+static size_t p2_smem() {
+  return (size_t)(P2Cta<T>::elems / L) * P2<L>::RS * sizeof(cplx<T>);
+}
+
 template <typename T>
 void dft_forward(const TransformDims& d, const FftPlan& px, const FftPlan& py, const T* phys, double2* spec,
                  int planes, void* work, cudaStream_t s) {
   using C = cplx<T>;
   C* w = reinterpret_cast<C*>(work);
   {
-    int nb = pick_nb(px.L, sizeof(C));
-    size_t sm = 2 * (size_t)nb * px.L * sizeof(C);
-    dim3 grid((d.ny + 2 * nb - 1) / (2 * nb), planes);
-    const PlanArgs pa = plan_args(px);
-    const C* tw = Tw<T>::get(px);
     prof_begin(s, PC_FFT_FX, (double)planes * d.ny * (d.nx * sizeof(T) + d.nxh * sizeof(C)), 0);
-#define TG_CALL(LC) fwd_x_kernel<T, LC><<<grid, 256, sm, s>>>(d, pa, tw, phys, w, nb)
-    TG_FFT_DISPATCH(px.L, TG_CALL)
+    const C* tw = Tw<T>::get(px);
+    if (p2_length(px.L)) {
+#define TG_CALL(LL)                                                                         \
+  {                                                                                         \
+    constexpr int NB = P2Cta<T>::elems / LL;                                                \
+    dim3 grid((d.ny + 2 * NB - 1) / (2 * NB), planes);                                      \
+    fx_p2_kernel<T, LL, NB><<<grid, NB * LL / 16, p2_smem<T, LL>(), s>>>(d, tw, phys, w);   \
+  }
+      TG_P2_DISPATCH(px.L, TG_CALL)
 #undef TG_CALL
+    } else {
+      int nb = pick_nb(px.L, sizeof(C));
+      size_t sm = 2 * (size_t)nb * px.L * sizeof(C);
+      dim3 grid((d.ny + 2 * nb - 1) / (2 * nb), planes);
+      const PlanArgs pa = plan_args(px);
+      fwd_x_kernel<T, 0><<<grid, 256, sm, s>>>(d, pa, tw, phys, w, nb);
+    }
     prof_end(s);
     TG_LAUNCH_CHECK("fwd_x_kernel");
   }
   {
-    int nb = pick_nb(py.L, sizeof(C));
-    size_t sm = 2 * (size_t)nb * py.L * sizeof(C);
-    dim3 grid((d.nxh + nb - 1) / nb, planes);
-    const PlanArgs pa = plan_args(py);
-    const C* tw = Tw<T>::get(py);
     const double scale = 1.0 / ((double)d.nx * (double)d.ny);
     prof_begin(s, PC_FFT_FY, (double)planes * ((double)d.nxh * d.ny * sizeof(C) + (double)d.M * sizeof(double2)), 0);
-#define TG_CALL(LC) fwd_y_kernel<T, LC><<<grid, 256, sm, s>>>(d, pa, tw, w, spec, nb, scale)
-    TG_FFT_DISPATCH(py.L, TG_CALL)
+    const C* tw = Tw<T>::get(py);
+    if (p2_length(py.L)) {
+#define TG_CALL(LL)                                                                              \
+  {                                                                                              \
+    constexpr int NB = P2Cta<T>::elems / LL;                                                     \
+    dim3 grid((d.nxh + NB - 1) / NB, planes);                                                    \
+    fy_p2_kernel<T, LL, NB><<<grid, NB * LL / 16, p2_smem<T, LL>(), s>>>(d, tw, w, spec, scale); \
+  }
+      TG_P2_DISPATCH(py.L, TG_CALL)
 #undef TG_CALL
+    } else {
+      int nb = pick_nb(py.L, sizeof(C));
+      size_t sm = 2 * (size_t)nb * py.L * sizeof(C);
+      dim3 grid((d.nxh + nb - 1) / nb, planes);
+      const PlanArgs pa = plan_args(py);
+      fwd_y_kernel<T, 0><<<grid, 256, sm, s>>>(d, pa, tw, w, spec, nb, scale);
+    }
     prof_end(s);
     TG_LAUNCH_CHECK("fwd_y_kernel");
   }
@@ -500,28 +759,46 @@ void dft_backward(const TransformDims& d, const FftPlan& px, const FftPlan& py, 
   using C = cplx<T>;
   C* w = reinterpret_cast<C*>(work);
   {
-    int nb = pick_nb(py.L, sizeof(C));
-    size_t sm = 2 * (size_t)nb * py.L * sizeof(C);
-    dim3 grid((d.nxh + nb - 1) / nb, planes);
-    const PlanArgs pa = plan_args(py);
-    const C* tw = Tw<T>::get(py);
     prof_begin(s, PC_FFT_BY, (double)planes * ((double)d.nxh * d.ny * sizeof(C) + (double)d.M * sizeof(double2)), 0);
-#define TG_CALL(LC) bwd_y_kernel<T, LC><<<grid, 256, sm, s>>>(d, pa, tw, spec, w, nb)
-    TG_FFT_DISPATCH(py.L, TG_CALL)
+    const C* tw = Tw<T>::get(py);
+    if (p2_length(py.L)) {
+#define TG_CALL(LL)                                                                       \
+  {                                                                                       \
+    constexpr int NB = P2Cta<T>::elems / LL;                                              \
+    dim3 grid((d.nxh + NB - 1) / NB, planes);                                             \
+    by_p2_kernel<T, LL, NB><<<grid, NB * LL / 16, p2_smem<T, LL>(), s>>>(d, tw, spec, w); \
+  }
+      TG_P2_DISPATCH(py.L, TG_CALL)
 #undef TG_CALL
+    } else {
+      int nb = pick_nb(py.L, sizeof(C));
+      size_t sm = 2 * (size_t)nb * py.L * sizeof(C);
+      dim3 grid((d.nxh + nb - 1) / nb, planes);
+      const PlanArgs pa = plan_args(py);
+      bwd_y_kernel<T, 0><<<grid, 256, sm, s>>>(d, pa, tw, spec, w, nb);
+    }
     prof_end(s);
     TG_LAUNCH_CHECK("bwd_y_kernel");
   }
   {
-    int nb = pick_nb(px.L, sizeof(C));
-    size_t sm = 2 * (size_t)nb * px.L * sizeof(C);
-    dim3 grid((d.ny + 2 * nb - 1) / (2 * nb), planes);
-    const PlanArgs pa = plan_args(px);
-    const C* tw = Tw<T>::get(px);
     prof_begin(s, PC_FFT_BX, (double)planes * d.ny * (d.nx * sizeof(T) + d.nxh * sizeof(C)), 0);
-#define TG_CALL(LC) bwd_x_kernel<T, LC><<<grid, 256, sm, s>>>(d, pa, tw, w, phys, nb)
-    TG_FFT_DISPATCH(px.L, TG_CALL)
+    const C* tw = Tw<T>::get(px);
+    if (p2_length(px.L)) {
+#define TG_CALL(LL)                                                                       \
+  {                                                                                       \
+    constexpr int NB = P2Cta<T>::elems / LL;                                              \
+    dim3 grid((d.ny + 2 * NB - 1) / (2 * NB), planes);                                    \
+    bx_p2_kernel<T, LL, NB><<<grid, NB * LL / 16, p2_smem<T, LL>(), s>>>(d, tw, w, phys); \
+  }
+      TG_P2_DISPATCH(px.L, TG_CALL)
 #undef TG_CALL
+    } else {
+      int nb = pick_nb(px.L, sizeof(C));
+      size_t sm = 2 * (size_t)nb * px.L * sizeof(C);
+      dim3 grid((d.ny + 2 * nb - 1) / (2 * nb), planes);
+      const PlanArgs pa = plan_args(px);
+      bwd_x_kernel<T, 0><<<grid, 256, sm, s>>>(d, pa, tw, w, phys, nb);
+    }
     prof_end(s);
     TG_LAUNCH_CHECK("bwd_x_kernel");
   }
