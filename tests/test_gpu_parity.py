@@ -51,10 +51,11 @@ def sediment_cfg(**kw):
 # ----------------------------------------------------------------------------
 # field-container primitives
 # ----------------------------------------------------------------------------
-# power-of-two lengths 8..1024 run the in-place radix-16 kernels, the others
-# the mixed-radix kernels; (256, 256, 129) spans several launches (chunks)
+# powers of two 8..1024 run the in-place radix-16 pass kernels, the other
+# lengths the mixed-radix pass kernels
 @pytest.mark.parametrize("shape", [(24, 18, 9), (32, 32, 17), (3, 3, 5), (30, 20, 7), (8, 8, 3), (16, 64, 3),
-                                   (1024, 16, 3), (8, 1024, 3), (128, 512, 3), (512, 24, 3), (256, 256, 129)])
+                                   (1024, 16, 3), (8, 1024, 3), (128, 512, 3), (512, 24, 3), (256, 256, 129),
+                                   (64, 64, 5), (256, 64, 3), (512, 128, 3), (64, 512, 3), (512, 256, 3)])
 def test_dft_f64_matches_oracle(cuda, shape):
     import torch
     nx, ny, nz = shape
@@ -77,7 +78,7 @@ def test_dft_f64_matches_oracle(cuda, shape):
 
 
 @pytest.mark.parametrize("shape", [(24, 18, 9), (64, 48, 5), (256, 256, 4), (1024, 8, 3), (16, 512, 3),
-                                   (32, 16, 3)])
+                                   (32, 16, 3), (64, 128, 5), (512, 256, 3), (128, 64, 9), (512, 512, 3)])
 def test_dft_f32_matches_oracle(cuda, shape):
     import torch
     nx, ny, nz = shape
@@ -194,6 +195,11 @@ def test_fp64_steps_with_sediment_sloped(cuda):
     _compare_run(cfg, 11, seed=5, noise=0.05, tol=1e-10)
 
 
+def test_fp64_steps_radix16_transforms(cuda):
+    """A 64 x 64 grid runs the in-place radix-16 transforms in every stage."""
+    _compare_run(sediment_cfg(nx=64, ny=64, nz=17), 2, seed=9, noise=0.05, tol=1e-10)
+
+
 def test_fp64_steps_native_decompositions(cuda):
     """Operators built by the library's own eigen-solver (no oracle matrices)."""
     _compare_run(sediment_cfg(nz=33), 3, seed=6, noise=0.05, tol=1e-9, oracle_dec=False, check_features=False)
@@ -228,8 +234,9 @@ def test_plugin_methods_match_run_steps(cuda):
     b.close()
 
 
-def test_mixed_precision_close_to_fp64(cuda):
-    cfg = sediment_cfg(nx=32, ny=32, nz=33)
+@pytest.mark.parametrize("n", [32, 64])
+def test_mixed_precision_close_to_fp64(cuda, n):
+    cfg = sediment_cfg(nx=n, ny=n, nz=33)
     uvw, p, phi = O.make_initial_state(cfg, seed=8, noise=0.05)
     f64 = gpu_case(cfg, "fp64")
     mx = gpu_case(cfg, "mixed")

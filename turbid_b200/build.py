@@ -11,6 +11,7 @@ import os
 import shutil
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
@@ -45,16 +46,22 @@ def build(verbose: bool = False, force: bool = False) -> str:
         return LIB
     os.makedirs(BUILD_DIR, exist_ok=True)
     nvcc = _nvcc()
-    objs = []
     common = ["-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
               "-lineinfo", "--expt-relaxed-constexpr"]
-    for s in srcs:
-        o = os.path.join(BUILD_DIR, os.path.basename(s) + ".o")
-        cmd = [nvcc, "-c", s, "-o", o] + ARCH + common
+    objs = [os.path.join(BUILD_DIR, os.path.basename(s) + ".o") for s in srcs]
+
+    def compile_one(src_obj):
+        src, obj = src_obj
+        if not force and _newer(obj, [src] + headers):
+            return
+        cmd = [nvcc, "-c", src, "-o", obj] + ARCH + common
         if verbose:
-            print(" ".join(cmd))
+            print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)
-        objs.append(o)
+
+    # translation units compile in parallel (the transform kernels dominate)
+    with ThreadPoolExecutor(max_workers=min(len(srcs), os.cpu_count() or 1)) as pool:
+        list(pool.map(compile_one, zip(srcs, objs)))
     cmd = [nvcc, "-shared", "-o", LIB] + objs + ARCH + ["-Xcompiler", "-fPIC"]
     if verbose:
         print(" ".join(cmd))

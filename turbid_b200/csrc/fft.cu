@@ -15,7 +15,7 @@
 #include <cstring>
 #include <mutex>
 
-#include "tg_common.cuh"
+#include "fft_dev.cuh"
 
 namespace tg {
 
@@ -69,17 +69,6 @@ static PlanArgs plan_args(const FftPlan& p) {
   a.npass = p.npass;
   for (int i = 0; i < kMaxPasses; ++i) a.rad[i] = p.rad[i];
   return a;
-}
-
-// ---------------------------------------------------------------------------
-// device FFT of NB transforms of length L held in shared memory
-// DIR = -1: exp(-i...) (forward), DIR = +1: exp(+i...) (backward, unscaled)
-// ---------------------------------------------------------------------------
-template <typename T, int DIR>
-__device__ __forceinline__ cplx<T> tw_get(const cplx<T>* tw, int idx) {
-  cplx<T> w = tw[idx];
-  if (DIR > 0) w.y = -w.y;
-  return w;
 }
 
 template <typename T, int DIR>
@@ -153,64 +142,6 @@ __device__ cplx<T>* fft_batch(cplx<T>* b0, cplx<T>* b1, int NB, const PlanArgs& 
 // while 16 divides the remaining length, then one radix-8/4/2 pass; the small
 // DFTs are even/odd splits with constant twiddles, all indexing constant-folded.
 // ---------------------------------------------------------------------------
-template <typename C, int DIR>
-__device__ __forceinline__ C rot(C a, double c, double s) {  // a * (c + i DIR s)
-  using R = decltype(C::x);
-  const R cr = (R)c, sr = (R)(DIR * s);
-  return mkc<C>(a.x * cr - a.y * sr, a.x * sr + a.y * cr);
-}
-
-// cos(2 pi i / 16); sin(2 pi i / 16) = cos16(i - 4)
-__host__ __device__ constexpr double cos16(int i) {
-  i &= 15;
-  if (i > 8) i = 16 - i;
-  return i == 0 ? 1.0
-       : i == 1 ? 0.92387953251128675613
-       : i == 2 ? 0.70710678118654752440
-       : i == 3 ? 0.38268343236508977173
-       : i == 4 ? 0.0
-       : i == 5 ? -0.38268343236508977173
-       : i == 6 ? -0.70710678118654752440
-       : i == 7 ? -0.92387953251128675613
-       : -1.0;
-}
-
-template <int R, int DIR, typename C>
-__device__ __forceinline__ void dft_ct(C* v) {
-  if constexpr (R == 1) {
-    return;
-  } else if constexpr (R == 2) {
-    C a = v[0], b = v[1];
-    v[0] = cadd(a, b);
-    v[1] = csub(a, b);
-  } else {
-    constexpr int H = R / 2;
-    C e[H], o[H];
-#pragma unroll
-    for (int m = 0; m < H; ++m) {
-      e[m] = v[2 * m];
-      o[m] = v[2 * m + 1];
-    }
-    dft_ct<H, DIR>(e);
-    dft_ct<H, DIR>(o);
-#pragma unroll
-    for (int k = 0; k < H; ++k) {
-      // W_R^k = cos(2 pi k/R) + i DIR sin(2 pi k/R) with DIR = -1 forward (R <= 16)
-      const int i16 = k * (16 / R);
-      C t;
-      if (k == 0) {
-        t = o[k];
-      } else if (4 * k == R) {
-        t = (DIR < 0) ? mkc<C>(o[k].y, -o[k].x) : mkc<C>(-o[k].y, o[k].x);
-      } else {
-        t = rot<C, DIR>(o[k], cos16(i16), cos16(i16 - 4));
-      }
-      v[k] = cadd(e[k], t);
-      v[k + H] = csub(e[k], t);
-    }
-  }
-}
-
 template <typename T, int DIR, int L, int Ns>
 __device__ __forceinline__ cplx<T>* ct_passes(cplx<T>* in, cplx<T>* out, int NB, const cplx<T>* __restrict__ tw) {
   using C = cplx<T>;
@@ -252,14 +183,6 @@ __device__ __forceinline__ cplx<T>* fft_any(cplx<T>* b0, cplx<T>* b1, int NB, co
   else
     return fft_batch<T, DIR>(b0, b1, NB, pl, tw);
 }
-
-template <typename T> struct Tw;
-template <> struct Tw<double> {
-  static __host__ const double2* get(const FftPlan& p) { return p.tw64; }
-};
-template <> struct Tw<float> {
-  static __host__ const float2* get(const FftPlan& p) { return p.tw32; }
-};
 
 // ---------------------------------------------------------------------------
 // forward x pass: phys [plane][y][x] (T) -> work [plane][kx][y] (cplx<T>)
@@ -405,72 +328,6 @@ __global__ void __launch_bounds__(256) bwd_x_kernel(TransformDims d, PlanArgs pl
     if (yb < d.ny) dst[(size_t)yb * d.nx + x] = z.y;
   }
 }
-
-// ---------------------------------------------------------------------------
-// Power-of-two lengths: in-place passes on one padded shared buffer.
-//
-// NB transforms of length L per CTA, NB*L/16 threads, every thread holding
-// 16 complex values of a pass in registers (one radix-16 butterfly, or 16/R
-// butterflies of a smaller final radix), so a pass reads all its inputs,
-// synchronises, and writes its outputs in place.  Shared rows are padded with
-// one spare slot per 16 values (index i -> i + i/16) and one more per row, so
-// the stride-16 writes of the first pass and the column accesses of the
-// x <-> y reorder hit distinct banks.
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ int sp(int i) { return i + (i >> 4); }
-
-template <int L> struct P2 {
-  static constexpr int RS = L + L / 16 + 1;  // padded row stride (complex values)
-};
-
-// complex values per CTA: 4096 in FP32, 2048 in FP64 (about 35 KB of shared memory)
-template <typename T> struct P2Cta {
-  static constexpr int elems = sizeof(T) == 4 ? 4096 : 2048;
-};
-
-template <typename T, int DIR, int L, int NB, int Ns>
-__device__ __forceinline__ void ip_passes(cplx<T>* buf, const cplx<T>* __restrict__ tw) {
-  using C = cplx<T>;
-  if constexpr (Ns < L) {
-    constexpr int rem = L / Ns;
-    constexpr int R = rem >= 16 ? 16 : rem;
-    constexpr int nb = L / R;          // butterflies per transform
-    constexpr int NT = NB * L / 16;    // threads of the CTA
-    constexpr int BPT = 16 / R;        // butterflies per thread
-    constexpr int RS = P2<L>::RS;
-    constexpr int twstep = L / (Ns * R);
-    C v[BPT][R];
-#pragma unroll
-    for (int t = 0; t < BPT; ++t) {
-      const int g = threadIdx.x + t * NT;
-      const int b = g / nb, j = g - b * nb;
-      const C* src = buf + b * RS;
-      const int jm = j % Ns;
-#pragma unroll
-      for (int r = 0; r < R; ++r) {
-        v[t][r] = src[sp(j + r * nb)];
-        if (Ns > 1 && r > 0) v[t][r] = cmul(v[t][r], tw_get<T, DIR>(tw, jm * r * twstep));
-      }
-      dft_ct<R, DIR>(v[t]);
-    }
-    __syncthreads();
-#pragma unroll
-    for (int t = 0; t < BPT; ++t) {
-      const int g = threadIdx.x + t * NT;
-      const int b = g / nb, j = g - b * nb;
-      const int jm = j % Ns;
-      const int base = (j - jm) * R + jm;
-      C* dst = buf + b * RS;
-#pragma unroll
-      for (int k = 0; k < R; ++k) dst[sp(base + k * Ns)] = v[t][k];
-    }
-    __syncthreads();
-    ip_passes<T, DIR, L, NB, Ns * R>(buf, tw);
-  }
-}
-
-// spectral row iy -> FFT index along y (P3DFFT pruning, reference src/base.cc:228-237)
-__device__ __forceinline__ int y_of(int iy, int ny, int nyc) { return iy < nyc / 2 ? iy : ny - (nyc - iy); }
 
 // forward x pass, L = nx: NB row pairs per CTA, 2 rows packed per complex FFT
 template <typename T, int L, int NB>
