@@ -415,6 +415,7 @@ static void carrier_predict(Ctx& x, int stage) {
     fwd<T>(x, prd, x.F6, 6 * x.nz);
     // adv_i = d/dx(u_i u) + d/dy(u_i v) + d/dz(u_i w): GradientTmp + sum
     const int inI[3] = {2, 4, 5}, x0I[3] = {0, 1, 2}, x1I[3] = {1, 3, 4};
+    ZProblem pr[3];
     for (int i = 0; i < 3; ++i) {
       EpiParams ep;
       ep.mode = EPI_DIV;
@@ -423,8 +424,9 @@ static void carrier_predict(Ctx& x, int stage) {
       ep.X0 = x.F6 + x0I[i] * S;
       ep.X1 = x.F6 + x1I[i] * S;
       ep.s = 1.0;
-      gemm(x, x.opD1, x.F6 + inI[i] * S, S, x.ADV + i * S, S, 1, ep);
+      pr[i] = ZProblem{&x.opD1, x.F6 + inI[i] * S, (long long)S, x.ADV + i * S, (long long)S, 1, ep};
     }
+    zgemm_group(pr, 3, x.M, x.s);
     // only the wall rows of du_i/dz are read in this form
     wall_dz(x.U, x.DU, S, x.M, x.nz, x.d1r0, x.d1rn, x.s);
   } else {
@@ -490,16 +492,22 @@ static void carrier_predict(Ctx& x, int stage) {
     boundary_apply(x.RHS, x.hist, S, x.M, x.nz, 2 * dt * c3m0, r, x.opentop ? 1 : 0, x.c.bc_u[4], x.c.bc_v[4],
                    x.c.bc_w[4], x.s);
   }
-  // Helmholtz, predict branch (phase_carrier_flat.cc:861-931)
-  for (int i = 0; i < 3; ++i) {
-    EpiParams ep;
-    ep.mode = EPI_RSCALE;
-    ep.lam = x.lamd[i];
-    ep.k2 = x.k2;
-    ep.sigma = x.sig_u[stage];
-    ep.null_mode = std::fabs(ep.sigma) < kSmall;
-    gemm(x, x.opEinv[i], x.RHS + i * S, S, x.TMP + i * S, S, 1, ep);
-    gemm(x, x.opE[i], x.TMP + i * S, S, x.SU + i * S, S, 1, EpiParams());
+  // Helmholtz, predict branch (phase_carrier_flat.cc:861-931): the three
+  // components' E^-1 products in one launch, then their E products
+  {
+    ZProblem fwd[3], bwd[3];
+    for (int i = 0; i < 3; ++i) {
+      EpiParams ep;
+      ep.mode = EPI_RSCALE;
+      ep.lam = x.lamd[i];
+      ep.k2 = x.k2;
+      ep.sigma = x.sig_u[stage];
+      ep.null_mode = std::fabs(ep.sigma) < kSmall;
+      fwd[i] = ZProblem{&x.opEinv[i], x.RHS + i * S, (long long)S, x.TMP + i * S, (long long)S, 1, ep};
+      bwd[i] = ZProblem{&x.opE[i], x.TMP + i * S, (long long)S, x.SU + i * S, (long long)S, 1, EpiParams()};
+    }
+    zgemm_group(fwd, 3, x.M, x.s);
+    zgemm_group(bwd, 3, x.M, x.s);
   }
 }
 

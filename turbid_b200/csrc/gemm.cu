@@ -24,6 +24,11 @@
 //          (j < h), Ae[i][h] = A[i][h], and  y[i] = P + Q, y[n-1-i] = s (P - Q)
 //          for i <= h: half the flops of the dense product.  CTA = MT*8 folded
 //          rows x 64 reals; each warp holds P and Q of one n-tile.
+//
+// A launch may carry up to kMaxGroup problems (different operators, inputs,
+// outputs and epilogues of the same kernel shape): blockIdx.z enumerates the
+// components of all of them, so independent z-solves share one grid and one
+// tail.
 #include <algorithm>
 #include <cmath>
 
@@ -106,14 +111,17 @@ struct GemmArgs {
   double* C;
   long long out_stride;
   int M;
+  int batch;          // components of this problem
   EpiParams ep;
 };
+
+constexpr int kMaxGroup = 3;
 
 // ---------------------------------------------------------------------------
 // dense: out rows [r0, r0 + 8*MT), columns [j0, j0 + 128) reals
 // ---------------------------------------------------------------------------
 template <int MT>
-__global__ void __launch_bounds__(kThreads) zgemm_dense_kernel(GemmArgs g) {
+__device__ __forceinline__ void dense_body(const GemmArgs& g, const int b) {
   constexpr int BM = 8 * MT, BN = 128, BST = BN + 4;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double* As = reinterpret_cast<double*>(smem_raw);   // [2][BM][AST]
@@ -121,7 +129,6 @@ __global__ void __launch_bounds__(kThreads) zgemm_dense_kernel(GemmArgs g) {
   const int ncol = 2 * g.M;
   const int r0 = blockIdx.x * BM;
   const int j0 = blockIdx.y * BN;
-  const int b = blockIdx.z;
   const double* Bb = g.B + (size_t)b * g.in_stride * 2;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int nkt = (g.K + BK - 1) / BK;
@@ -205,7 +212,7 @@ __global__ void __launch_bounds__(kThreads) zgemm_dense_kernel(GemmArgs g) {
 // sym: folded rows [r0, r0 + 8*MT) of P and Q, columns [j0, j0 + 64) reals
 // ---------------------------------------------------------------------------
 template <int MT>
-__global__ void __launch_bounds__(kThreads) zgemm_sym_kernel(GemmArgs g) {
+__device__ __forceinline__ void sym_body(const GemmArgs& g, const int b) {
   constexpr int BM = 8 * MT, BN = 64, BST = BN + 4;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double* Ae = reinterpret_cast<double*>(smem_raw);   // [2][BM][AST]
@@ -216,7 +223,6 @@ __global__ void __launch_bounds__(kThreads) zgemm_sym_kernel(GemmArgs g) {
   const int n = g.nz, h = (g.nz - 1) / 2;
   const int r0 = blockIdx.x * BM;
   const int j0 = blockIdx.y * BN;
-  const int b = blockIdx.z;
   const double* Bb = g.B + (size_t)b * g.in_stride * 2;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int nkt = (g.K + BK - 1) / BK;
@@ -324,6 +330,38 @@ __global__ void __launch_bounds__(kThreads) zgemm_sym_kernel(GemmArgs g) {
   }
 }
 
+// blockIdx.z runs over the components of all problems of the launch (NP = 1
+// or kMaxGroup; unused trailing problems have batch 0).  The problems are
+// separate by-value parameters so that each body reads its arguments as
+// constant-bank operands.
+#define TG_GROUP_DISPATCH(BODY)               \
+  int z = blockIdx.z;                         \
+  if (NP == 1 || z < g0.batch) {              \
+    BODY(g0, z);                              \
+    return;                                   \
+  }                                           \
+  z -= g0.batch;                              \
+  if (z < g1.batch) {                         \
+    BODY(g1, z);                              \
+    return;                                   \
+  }                                           \
+  z -= g1.batch;                              \
+  BODY(g2, z);
+
+template <int MT, int NP>
+__global__ void __launch_bounds__(kThreads) zgemm_dense_kernel(GemmArgs g0, GemmArgs g1, GemmArgs g2) {
+#define TG_BODY(G, Z) dense_body<MT>(G, Z)
+  TG_GROUP_DISPATCH(TG_BODY)
+#undef TG_BODY
+}
+
+template <int MT, int NP>
+__global__ void __launch_bounds__(kThreads) zgemm_sym_kernel(GemmArgs g0, GemmArgs g1, GemmArgs g2) {
+#define TG_BODY(G, Z) sym_body<MT>(G, Z)
+  TG_GROUP_DISPATCH(TG_BODY)
+#undef TG_BODY
+}
+
 template <int MT>
 size_t dense_smem() {
   return 2 * (8 * MT * AST + BK * (128 + 4)) * sizeof(double);
@@ -333,68 +371,114 @@ size_t sym_smem() {
   return 2 * (2 * 8 * MT * AST + 2 * BK * (64 + 4)) * sizeof(double);
 }
 
+constexpr int kMaxMtDense = 16, kMaxMtSym = 16;
 #define TG_MT_LIST(X) X(1) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12) X(13) X(14) X(15) X(16)
+#define TG_MT_SYM_LIST(X) TG_MT_LIST(X)
 
 }  // namespace
 
 void zgemm_init() {
 #define TG_SET(MT)                                                                                           \
-  TG_CUDA(cudaFuncSetAttribute(zgemm_dense_kernel<MT>, cudaFuncAttributeMaxDynamicSharedMemorySize,         \
+  TG_CUDA(cudaFuncSetAttribute(zgemm_dense_kernel<MT, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,      \
                                (int)dense_smem<MT>()));                                                      \
-  TG_CUDA(cudaFuncSetAttribute(zgemm_sym_kernel<MT>, cudaFuncAttributeMaxDynamicSharedMemorySize,           \
-                               (int)sym_smem<MT>()));
+  TG_CUDA(cudaFuncSetAttribute(zgemm_dense_kernel<MT, kMaxGroup>,                                           \
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dense_smem<MT>()));
   TG_MT_LIST(TG_SET)
+#undef TG_SET
+#define TG_SET(MT)                                                                                           \
+  TG_CUDA(cudaFuncSetAttribute(zgemm_sym_kernel<MT, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,        \
+                               (int)sym_smem<MT>()));                                                        \
+  TG_CUDA(cudaFuncSetAttribute(zgemm_sym_kernel<MT, kMaxGroup>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                               (int)sym_smem<MT>()));
+  TG_MT_SYM_LIST(TG_SET)
 #undef TG_SET
 }
 
-// m-tiles per CTA for `rows` rows: as few row tiles as possible with at most 16
-// m-tiles each, then the tiles as even as possible
-void row_tiling(int rows, int& mt, int& tiles) {
+// m-tiles per CTA for `rows` rows: as few row tiles as possible with at most
+// maxmt m-tiles each, then the tiles as even as possible
+void row_tiling(int rows, int maxmt, int& mt, int& tiles) {
   const int need = (rows + 7) / 8;
-  tiles = (need + 15) / 16;
+  tiles = (need + maxmt - 1) / maxmt;
   mt = (need + tiles - 1) / tiles;
 }
 
-void zgemm(const ZOperator& op, const double2* in, long long in_stride, double2* out, long long out_stride, int M,
-           int batch, const EpiParams& ep, cudaStream_t s) {
-  GemmArgs g;
-  g.lda = op.lda;
-  g.nz = op.n;
-  g.B = reinterpret_cast<const double*>(in);
-  g.in_stride = in_stride;
-  g.C = reinterpret_cast<double*>(out);
-  g.out_stride = out_stride;
-  g.M = M;
-  g.ep = ep;
-  // flops executed (the folded product does two (h+1)^2 halves), bytes in + out + operator
-  const double fl = (op.sym ? 2.0 * 4.0 * op.rows * op.rows : 4.0 * op.n * op.n) * (double)M * batch;
-  const double by = (double)batch * 16.0 * M * 2 * op.n + 8.0 * op.n * op.n;
+void zgemm_group(const ZProblem* probs, int nprob, int M, cudaStream_t s) {
+  if (nprob < 1 || nprob > kMaxGroup) throw Error{TG_ERR_ARG, "zgemm > bad group size"};
+  const ZOperator& op0 = *probs[0].op;
+  GemmArgs grp[kMaxGroup];
+  int total = 0;
+  double fl = 0.0, by = 0.0;
+  for (int i = 0; i < nprob; ++i) {
+    const ZProblem& pr = probs[i];
+    const ZOperator& op = *pr.op;
+    if (op.sym != op0.sym || op.mt != op0.mt || op.tiles != op0.tiles || op.n != op0.n)
+      throw Error{TG_ERR_ARG, "zgemm > operators of one launch differ in shape"};
+    GemmArgs& g = grp[i];
+    g.lda = op.lda;
+    g.nz = op.n;
+    g.B = reinterpret_cast<const double*>(pr.in);
+    g.in_stride = pr.in_stride;
+    g.C = reinterpret_cast<double*>(pr.out);
+    g.out_stride = pr.out_stride;
+    g.M = M;
+    g.batch = pr.batch;
+    g.ep = pr.ep;
+    g.ep.nz = op.n;
+    g.ep.M = M;
+    if (op.sym) {
+      g.A = op.Ae;
+      g.Ao = op.Ao;
+      g.rows = op.rows;
+      g.K = op.rows;
+      g.sgn = op.sgn;
+    } else {
+      g.A = op.A;
+      g.Ao = nullptr;
+      g.rows = op.n;
+      g.K = op.n;
+      g.sgn = 1;
+    }
+    total += pr.batch;
+    // flops executed (the folded product does two (h+1)^2 halves), bytes in + out + operator
+    fl += (op.sym ? 2.0 * 4.0 * op.rows * op.rows : 4.0 * op.n * op.n) * (double)M * pr.batch;
+    by += (double)pr.batch * 16.0 * M * 2 * op.n + 8.0 * op.n * op.n;
+  }
+  for (int i = nprob; i < kMaxGroup; ++i) {
+    grp[i] = grp[0];
+    grp[i].batch = 0;
+  }
   prof_begin(s, PC_GEMM, by, fl);
-  if (op.sym) {
-    g.A = op.Ae;
-    g.Ao = op.Ao;
-    g.rows = op.rows;
-    g.K = op.rows;
-    g.sgn = op.sgn;
-    dim3 grid(op.tiles, (2 * M + 63) / 64, batch);
-#define TG_CASE(MT) \
-  case MT: zgemm_sym_kernel<MT><<<grid, kThreads, sym_smem<MT>(), s>>>(g); break;
-    switch (op.mt) { TG_MT_LIST(TG_CASE) default: throw Error{TG_ERR_ARG, "zgemm > bad tiling"}; }
+  if (op0.sym) {
+    dim3 grid(op0.tiles, (2 * M + 63) / 64, total);
+#define TG_CASE(MT)                                                                                     \
+  case MT:                                                                                              \
+    if (nprob == 1)                                                                                     \
+      zgemm_sym_kernel<MT, 1><<<grid, kThreads, sym_smem<MT>(), s>>>(grp[0], grp[1], grp[2]);          \
+    else                                                                                                \
+      zgemm_sym_kernel<MT, kMaxGroup><<<grid, kThreads, sym_smem<MT>(), s>>>(grp[0], grp[1], grp[2]);  \
+    break;
+    switch (op0.mt) { TG_MT_SYM_LIST(TG_CASE) default: throw Error{TG_ERR_ARG, "zgemm > bad tiling"}; }
 #undef TG_CASE
   } else {
-    g.A = op.A;
-    g.Ao = nullptr;
-    g.rows = op.n;
-    g.K = op.n;
-    g.sgn = 1;
-    dim3 grid(op.tiles, (2 * M + 127) / 128, batch);
-#define TG_CASE(MT) \
-  case MT: zgemm_dense_kernel<MT><<<grid, kThreads, dense_smem<MT>(), s>>>(g); break;
-    switch (op.mt) { TG_MT_LIST(TG_CASE) default: throw Error{TG_ERR_ARG, "zgemm > bad tiling"}; }
+    dim3 grid(op0.tiles, (2 * M + 127) / 128, total);
+#define TG_CASE(MT)                                                                                       \
+  case MT:                                                                                                \
+    if (nprob == 1)                                                                                       \
+      zgemm_dense_kernel<MT, 1><<<grid, kThreads, dense_smem<MT>(), s>>>(grp[0], grp[1], grp[2]);        \
+    else                                                                                                  \
+      zgemm_dense_kernel<MT, kMaxGroup><<<grid, kThreads, dense_smem<MT>(), s>>>(grp[0], grp[1], grp[2]); \
+    break;
+    switch (op0.mt) { TG_MT_LIST(TG_CASE) default: throw Error{TG_ERR_ARG, "zgemm > bad tiling"}; }
 #undef TG_CASE
   }
   prof_end(s);
   TG_LAUNCH_CHECK("zgemm kernel");
+}
+
+void zgemm(const ZOperator& op, const double2* in, long long in_stride, double2* out, long long out_stride, int M,
+           int batch, const EpiParams& ep, cudaStream_t s) {
+  ZProblem p{&op, in, in_stride, out, out_stride, batch, ep};
+  zgemm_group(&p, 1, M, s);
 }
 
 // Upload an nz x nz operator: the dense copy always; the folded halves when
@@ -404,11 +488,11 @@ void zop_build(ZOperator& op, const std::vector<double>& A, int n, bool allow_sy
                const std::function<double*(size_t)>& alloc) {
   op.n = n;
   op.lda = (n + 15) / 16 * 16;
-  row_tiling(n, op.mt_dense, op.tiles_dense);
+  row_tiling(n, kMaxMtDense, op.mt_dense, op.tiles_dense);
   const int h = (n - 1) / 2;
   const int hr = h + 1;   // folded rows
   int mts, ts;
-  row_tiling(hr, mts, ts);
+  row_tiling(hr, kMaxMtSym, mts, ts);
   const int rowsAlloc = std::max(op.tiles_dense * op.mt_dense * 8, ts * mts * 8);
   if (op.rowsPad == 0) op.rowsPad = rowsAlloc;
   if (op.rowsPad < rowsAlloc) throw Error{TG_ERR_ARG, "zop_build > operator buffer too small"};

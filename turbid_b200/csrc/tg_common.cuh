@@ -150,11 +150,25 @@ struct ZOperator {
   double* Ao = nullptr;
 };
 
+// One problem of a grouped launch: batch components of `in` (stride in_stride
+// complex) through op into `out`, with its own epilogue.
+struct ZProblem {
+  const ZOperator* op;
+  const double2* in;
+  long long in_stride;
+  double2* out;
+  long long out_stride;
+  int batch;
+  EpiParams ep;
+};
+
 void zgemm_init();
-void row_tiling(int rows, int& mt, int& tiles);
+void row_tiling(int rows, int maxmt, int& mt, int& tiles);
 void zop_build(ZOperator& op, const std::vector<double>& A, int n, bool allow_sym,
                const std::function<double*(size_t)>& alloc);
 void zgemm(const ZOperator& op, const double2* in, long long in_stride, double2* out, long long out_stride, int M,
            int batch, const EpiParams& ep, cudaStream_t s);
+// up to three problems whose operators share the kernel shape, in one launch
+void zgemm_group(const ZProblem* probs, int nprob, int M, cudaStream_t s);
 
 }  // namespace tg
