@@ -209,81 +209,62 @@ __device__ __forceinline__ void dense_body(const GemmArgs& g, const int b) {
 }
 
 // ---------------------------------------------------------------------------
-// sym: folded rows [r0, r0 + 8*MT) of P and Q, columns [j0, j0 + 64) reals
+// sym: folded rows [r0, r0 + 8*MT) of P and Q, columns [j0, j0 + 128) reals
 // ---------------------------------------------------------------------------
 template <int MT>
 __device__ __forceinline__ void sym_body(const GemmArgs& g, const int b) {
-  constexpr int BM = 8 * MT, BN = 64, BST = BN + 4;
+  constexpr int BM = 8 * MT, BN = 128, BST = BN + 4;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double* Ae = reinterpret_cast<double*>(smem_raw);   // [2][BM][AST]
   double* Ao = Ae + 2 * BM * AST;                      // [2][BM][AST]
-  double* Be = Ao + 2 * BM * AST;                      // [2][BK][BST]
-  double* Bo = Be + 2 * BK * BST;                      // [2][BK][BST]
+  double* Bt = Ao + 2 * BM * AST;                      // [2][BK][BST] input rows k (k <= h)
+  double* Bb = Bt + 2 * BK * BST;                      // [2][BK][BST] input rows n-1-k (k < h, else 0)
   const int ncol = 2 * g.M;
   const int n = g.nz, h = (g.nz - 1) / 2;
   const int r0 = blockIdx.x * BM;
   const int j0 = blockIdx.y * BN;
-  const double* Bb = g.B + (size_t)b * g.in_stride * 2;
+  const double* Bsrc = g.B + (size_t)b * g.in_stride * 2;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int nkt = (g.K + BK - 1) / BK;
   int mt_valid = (g.rows - r0 + 7) / 8;
   mt_valid = mt_valid > MT ? MT : mt_valid;
 
-  // B tile: BK folded rows x 64 reals = 512 double2 per parity, 2 per thread
-  constexpr int BPT = (BK * BN / 2) / kThreads;
-  double2 lo[BPT], hi[BPT];
-  auto fetch_b = [&](int kt) {
-    const int k0 = kt * BK;
-#pragma unroll
-    for (int i = 0; i < BPT; ++i) {
-      int c = tid + i * kThreads;
-      int kr = c / (BN / 2), jj = (c % (BN / 2)) * 2;
-      int k = k0 + kr, j = j0 + jj;
-      lo[i] = make_double2(0.0, 0.0);
-      hi[i] = make_double2(0.0, 0.0);
-      if (k <= h && j < ncol) {
-        lo[i] = *reinterpret_cast<const double2*>(Bb + (size_t)k * ncol + j);
-        if (k < h) hi[i] = *reinterpret_cast<const double2*>(Bb + (size_t)(n - 1 - k) * ncol + j);
-      }
-    }
-  };
-  auto store_b = [&](int buf) {
-    double* be = Be + buf * BK * BST;
-    double* bo = Bo + buf * BK * BST;
-#pragma unroll
-    for (int i = 0; i < BPT; ++i) {
-      int c = tid + i * kThreads;
-      int kr = c / (BN / 2), jj = (c % (BN / 2)) * 2;
-      *reinterpret_cast<double2*>(be + kr * BST + jj) = make_double2(lo[i].x + hi[i].x, lo[i].y + hi[i].y);
-      *reinterpret_cast<double2*>(bo + kr * BST + jj) = make_double2(lo[i].x - hi[i].x, lo[i].y - hi[i].y);
-    }
-  };
-  auto load_a = [&](int kt, int buf) {
+  auto load_tile = [&](int kt, int buf) {
     const int k0 = kt * BK;
     double* ae = Ae + buf * BM * AST;
     double* ao = Ao + buf * BM * AST;
     for (int c = tid; c < BM * (BK / 2); c += kThreads) {
-      int row = c / (BK / 2), kk = (c % (BK / 2)) * 2;
+      const int row = c / (BK / 2), kk = (c % (BK / 2)) * 2;
       cp_async16(ae + row * AST + kk, g.A + (size_t)(r0 + row) * g.lda + k0 + kk, true);
       cp_async16(ao + row * AST + kk, g.Ao + (size_t)(r0 + row) * g.lda + k0 + kk, true);
     }
+    double* bt = Bt + buf * BK * BST;
+    double* bb = Bb + buf * BK * BST;
+#pragma unroll
+    for (int i = 0; i < (BK * BN / 2) / kThreads; ++i) {
+      const int c = tid + i * kThreads;
+      const int kr = c / (BN / 2), jj = (c % (BN / 2)) * 2;
+      const int k = k0 + kr, j = j0 + jj;
+      const bool okt = (k <= h) && (j < ncol);
+      const bool okb = (k < h) && (j < ncol);
+      cp_async16(bt + kr * BST + jj, okt ? Bsrc + (size_t)k * ncol + j : Bsrc, okt);
+      cp_async16(bb + kr * BST + jj, okb ? Bsrc + (size_t)(n - 1 - k) * ncol + j : Bsrc, okb);
+    }
   };
 
-  double accE[MT][2], accO[MT][2];
+  double accE[MT][2][2], accO[MT][2][2];
 #pragma unroll
-  for (int i = 0; i < MT; ++i) accE[i][0] = accE[i][1] = accO[i][0] = accO[i][1] = 0.0;
+  for (int i = 0; i < MT; ++i)
+#pragma unroll
+    for (int j = 0; j < 2; ++j) accE[i][j][0] = accE[i][j][1] = accO[i][j][0] = accO[i][j][1] = 0.0;
 
-  load_a(0, 0);
+  load_tile(0, 0);
   cp_async_commit();
-  fetch_b(0);
-  store_b(0);
   for (int kt = 0; kt < nkt; ++kt) {
     const int buf = kt & 1;
-    const bool more = kt + 1 < nkt;
-    if (more) {
-      load_a(kt + 1, buf ^ 1);
+    if (kt + 1 < nkt) {
+      load_tile(kt + 1, buf ^ 1);
       cp_async_commit();
-      fetch_b(kt + 1);   // global loads in flight during this tile's math
       cp_async_wait<1>();
     } else {
       cp_async_wait<0>();
@@ -291,25 +272,33 @@ __device__ __forceinline__ void sym_body(const GemmArgs& g, const int b) {
     __syncthreads();
     const double* ae = Ae + buf * BM * AST;
     const double* ao = Ao + buf * BM * AST;
-    const double* be = Be + buf * BK * BST;
-    const double* bo = Bo + buf * BK * BST;
+    const double* bt = Bt + buf * BK * BST;
+    const double* bb = Bb + buf * BK * BST;
     const int ksteps = min(BK / 4, (g.K - kt * BK + 3) / 4);
 #pragma unroll
     for (int ks = 0; ks < BK / 4; ++ks) {
       if (ks < ksteps) {
-        const int bi = (ks * 4 + (lane & 3)) * BST + warp * 8 + (lane >> 2);
-        const double bfe = be[bi], bfo = bo[bi];
+        double be[2], bo[2];
+#pragma unroll
+        for (int nt = 0; nt < 2; ++nt) {
+          const int bi = (ks * 4 + (lane & 3)) * BST + warp * 16 + nt * 8 + (lane >> 2);
+          const double top = bt[bi], bot = bb[bi];
+          be[nt] = top + bot;
+          bo[nt] = top - bot;
+        }
 #pragma unroll
         for (int mt = 0; mt < MT; ++mt) {
           if (mt < mt_valid) {
             const int ai = (mt * 8 + (lane >> 2)) * AST + ks * 4 + (lane & 3);
-            dmma(accE[mt][0], accE[mt][1], ae[ai], bfe);
-            dmma(accO[mt][0], accO[mt][1], ao[ai], bfo);
+            const double fe = ae[ai], fo = ao[ai];
+            dmma(accE[mt][0][0], accE[mt][0][1], fe, be[0]);
+            dmma(accE[mt][1][0], accE[mt][1][1], fe, be[1]);
+            dmma(accO[mt][0][0], accO[mt][0][1], fo, bo[0]);
+            dmma(accO[mt][1][0], accO[mt][1][1], fo, bo[1]);
           }
         }
       }
     }
-    if (more) store_b(buf ^ 1);   // its last readers finished before the barrier above
     __syncthreads();
   }
 
@@ -319,13 +308,16 @@ __device__ __forceinline__ void sym_body(const GemmArgs& g, const int b) {
   for (int mt = 0; mt < MT; ++mt) {
     const int i = r0 + mt * 8 + (lane >> 2);
     if (i > h) continue;
-    const int m = (j0 + warp * 8) / 2 + (lane & 3);
-    if (m >= g.M) continue;
-    const double pe = accE[mt][0], pi = accE[mt][1], qe = accO[mt][0], qi = accO[mt][1];
-    Cb[(size_t)i * g.M + m] = epilogue(g.ep, b, i, m, make_double2(pe + qe, pi + qi));
-    if (i < h) {
-      const int j = n - 1 - i;
-      Cb[(size_t)j * g.M + m] = epilogue(g.ep, b, j, m, make_double2(s * (pe - qe), s * (pi - qi)));
+#pragma unroll
+    for (int nt = 0; nt < 2; ++nt) {
+      const int m = (j0 + warp * 16 + nt * 8) / 2 + (lane & 3);
+      if (m >= g.M) continue;
+      const double pe = accE[mt][nt][0], pi = accE[mt][nt][1], qe = accO[mt][nt][0], qi = accO[mt][nt][1];
+      Cb[(size_t)i * g.M + m] = epilogue(g.ep, b, i, m, make_double2(pe + qe, pi + qi));
+      if (i < h) {
+        const int j = n - 1 - i;
+        Cb[(size_t)j * g.M + m] = epilogue(g.ep, b, j, m, make_double2(s * (pe - qe), s * (pi - qi)));
+      }
     }
   }
 }
@@ -356,7 +348,7 @@ __global__ void __launch_bounds__(kThreads) zgemm_dense_kernel(GemmArgs g0, Gemm
 }
 
 template <int MT, int NP>
-__global__ void __launch_bounds__(kThreads) zgemm_sym_kernel(GemmArgs g0, GemmArgs g1, GemmArgs g2) {
+__global__ void __launch_bounds__(kThreads, 2) zgemm_sym_kernel(GemmArgs g0, GemmArgs g1, GemmArgs g2) {
 #define TG_BODY(G, Z) sym_body<MT>(G, Z)
   TG_GROUP_DISPATCH(TG_BODY)
 #undef TG_BODY
@@ -368,12 +360,12 @@ size_t dense_smem() {
 }
 template <int MT>
 size_t sym_smem() {
-  return 2 * (2 * 8 * MT * AST + 2 * BK * (64 + 4)) * sizeof(double);
+  return 2 * (2 * 8 * MT * AST + 2 * BK * (128 + 4)) * sizeof(double);
 }
 
-constexpr int kMaxMtDense = 16, kMaxMtSym = 16;
+constexpr int kMaxMtDense = 16, kMaxMtSym = 6;
 #define TG_MT_LIST(X) X(1) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12) X(13) X(14) X(15) X(16)
-#define TG_MT_SYM_LIST(X) TG_MT_LIST(X)
+#define TG_MT_SYM_LIST(X) X(1) X(2) X(3) X(4) X(5) X(6)
 
 }  // namespace
 
@@ -449,7 +441,7 @@ void zgemm_group(const ZProblem* probs, int nprob, int M, cudaStream_t s) {
   }
   prof_begin(s, PC_GEMM, by, fl);
   if (op0.sym) {
-    dim3 grid(op0.tiles, (2 * M + 63) / 64, total);
+    dim3 grid(op0.tiles, (2 * M + 127) / 128, total);
 #define TG_CASE(MT)                                                                                     \
   case MT:                                                                                              \
     if (nprob == 1)                                                                                     \
