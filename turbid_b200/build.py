@@ -19,6 +19,9 @@ LIB = os.path.join(HERE, "libturbid_gpu.so")
 BUILD_DIR = os.path.join(HERE, "_build")
 
 CU_SOURCES = ["api.cu", "fft.cu", "gemm.cu", "fields.cu"]
+DRIVER_SRC = os.path.join(HERE, "host", "channelflat_gpu.cc")
+DRIVER = os.path.join(HERE, "channelflat_gpu")
+INCLUDE = os.path.join(HERE, "..", "include")
 CC_SOURCES = ["setup.cc"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
@@ -43,6 +46,7 @@ def build(verbose: bool = False, force: bool = False) -> str:
     headers = [os.path.join(CSRC, h) for h in os.listdir(CSRC) if h.endswith((".h", ".cuh"))]
     headers.append(os.path.join(HERE, "..", "include", "turbid_gpu.h"))
     if not force and _newer(LIB, srcs + headers):
+        build_driver(verbose=verbose)
         return LIB
     os.makedirs(BUILD_DIR, exist_ok=True)
     nvcc = _nvcc()
@@ -66,7 +70,22 @@ def build(verbose: bool = False, force: bool = False) -> str:
     if verbose:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)
+    build_driver(verbose=verbose, force=True)
     return LIB
+
+
+def build_driver(verbose: bool = False, force: bool = False) -> str:
+    """The C++ main program over the plugin classes (include/turbid_plugin.hpp)."""
+    deps = [DRIVER_SRC, LIB, os.path.join(INCLUDE, "turbid_plugin.hpp"), os.path.join(INCLUDE, "turbid_gpu.h")]
+    if not force and _newer(DRIVER, deps):
+        return DRIVER
+    cxx = shutil.which("g++") or "c++"
+    cmd = [cxx, "-O2", "-std=c++17", "-Wall", "-I", INCLUDE, DRIVER_SRC, "-L", HERE, "-lturbid_gpu",
+           "-Wl,-rpath,$ORIGIN", "-o", DRIVER]
+    if verbose:
+        print(" ".join(cmd))
+    subprocess.run(cmd, check=True)
+    return DRIVER
 
 
 if __name__ == "__main__":

@@ -1,0 +1,58 @@
+// The reference's main program (main/channelflat.cc) with the GPU plugin
+// classes: reads configuration.ini (or argv[1]) and the restart files of
+// task_start_step, runs the RK3 steps on the GPU, writes the restart files
+// every result_write_interval steps and one log line per step.
+//
+//   channelflat_gpu [configuration.ini [logcomputation]] [--mixed]
+//   channelflat_gpu --parse-only configuration.ini    (case parameters as JSON, no GPU)
+#include <iostream>
+#include <string>
+
+#include "turbid_plugin.hpp"
+
+namespace {
+void PrintCaseJson(const tg_case& c, const turbid::RunControl& rc) {
+  auto vec = [](const double* v, int n) {
+    std::ostringstream s;
+    s << "[";
+    for (int i = 0; i < n; ++i) s << (i ? ", " : "") << std::setprecision(17) << v[i];
+    s << "]";
+    return s.str();
+  };
+  std::ostringstream s;
+  s << std::setprecision(17) << "{\"nx\": " << c.nx << ", \"ny\": " << c.ny << ", \"nz\": " << c.nz
+    << ", \"lx\": " << c.lx << ", \"ly\": " << c.ly << ", \"nphase\": " << c.nphase << ", \"mapping\": " << c.mapping
+    << ", \"mapping_coef\": " << c.mapping_coef << ", \"slope\": " << c.slope
+    << ", \"slope_direction\": " << c.slope_direction << ", \"dt\": " << c.dt
+    << ", \"output_based_on_step\": " << c.output_based_on_step << ", \"reynolds\": " << c.reynolds
+    << ", \"froude\": " << c.froude << ", \"averaged_concentration\": " << c.averaged_concentration
+    << ", \"specific_gravity\": " << c.specific_gravity << ", \"affected_by_scalar\": " << c.affected_by_scalar
+    << ", \"bc_u\": " << vec(c.bc_u, 5) << ", \"bc_v\": " << vec(c.bc_v, 5) << ", \"bc_w\": " << vec(c.bc_w, 5)
+    << ", \"bc_p\": " << vec(c.bc_p, 5) << ", \"force_type\": " << c.force_type << ", \"force_direction\": ["
+    << c.force_direction[0] << ", " << c.force_direction[1] << "], \"force_amplitude\": " << vec(c.force_amplitude, 2)
+    << ", \"schmidt\": " << c.schmidt << ", \"settling\": " << c.settling << ", \"erosion_rate\": " << c.erosion_rate
+    << ", \"critical_shear\": " << c.critical_shear << ", \"scalar_bc\": " << c.scalar_bc
+    << ", \"maxcfl\": " << rc.maxcfl << ", \"maxstep\": " << rc.maxstep << ", \"writeinterval\": " << rc.writeinterval
+    << ", \"startstep\": " << rc.startstep << "}";
+  std::cout << s.str() << std::endl;
+}
+}  // namespace
+
+int main(int argc, char** argv) {
+  try {
+    if (argc > 2 && std::string(argv[1]) == "--parse-only") {
+      turbid::IniFile ini;
+      ini.Load(argv[2]);
+      turbid::RunControl rc;
+      PrintCaseJson(turbid::CaseFromIni(ini, rc), rc);
+      return 0;
+    }
+    turbid::FlatChannelSolver solver(argc, argv);
+    solver.Configure();
+    solver.Execute();
+  } catch (std::runtime_error& err) {
+    std::cout << err.what() << std::endl;
+    return 1;
+  }
+  return 0;
+}
