@@ -56,39 +56,79 @@ __device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b)
                : "d"(a), "d"(b));
 }
 
-__device__ __forceinline__ double2 epilogue(const EpiParams& ep, int b, int r, int m, double2 acc) {
-  switch (ep.mode) {
+// Epilogue in two phases: the operands of several outputs are loaded first
+// (the output stores may alias them as far as the compiler knows, so loads
+// issued after a store would each wait for it), then combined and stored.
+struct EpiIn {
+  double2 a, c;   // DIV: X0, X1; LAPRHS: H, U; GRAD: X
+  double s0, s1;  // DIV/GRAD: kx, ky; LAPRHS: dx2, dy2; RSCALE: k2 + lam (+ sigma), lam
+};
+
+template <int MODE>
+__device__ __forceinline__ EpiIn epi_load(const EpiParams& ep, int b, int r, int m) {
+  EpiIn in;
+  switch (MODE) {
+    case EPI_RSCALE:
+      if (r != 0 && r != ep.nz - 1) {
+        in.s1 = ep.lam[r];
+        in.s0 = (ep.k2[m] + in.s1) + ep.sigma;
+      }
+      break;
+    case EPI_DIV: {
+      const size_t o = (size_t)b * ep.sX + (size_t)r * ep.M + m;
+      in.a = ep.X0[o];
+      in.c = ep.X1[o];
+      in.s0 = ep.kx[m];
+      in.s1 = ep.ky[m];
+      break;
+    }
+    case EPI_LAPRHS:
+      in.a = ep.H[(size_t)b * ep.sH + (size_t)r * ep.M + m];
+      in.c = ep.U[(size_t)b * ep.sU + (size_t)r * ep.M + m];
+      in.s0 = ep.dx2[m];
+      in.s1 = ep.dy2[m];
+      break;
+    case EPI_GRAD:
+      in.a = ep.X0[(size_t)b * ep.sX + (size_t)r * ep.M + m];
+      in.s0 = ep.kx[m];
+      in.s1 = ep.ky[m];
+      break;
+    default:
+      break;
+  }
+  return in;
+}
+
+template <int MODE>
+__device__ __forceinline__ double2 epi_apply(const EpiParams& ep, int b, int r, int m, double2 acc, const EpiIn& in) {
+  switch (MODE) {
     case EPI_RSCALE: {
       double R = 1.0;
       if (r != 0 && r != ep.nz - 1) {
-        R = 1.0 / ((ep.k2[m] + ep.lam[r]) + ep.sigma);
-        if (ep.null_mode && m == 0 && fabs(ep.lam[r]) < 10e-12) R = 0.0;
+        R = 1.0 / in.s0;
+        if (ep.null_mode && m == 0 && fabs(in.s1) < 10e-12) R = 0.0;
       }
       return make_double2(acc.x * R, acc.y * R);
     }
     case EPI_DIV: {
-      const size_t o = (size_t)b * ep.sX + (size_t)r * ep.M + m;
-      double2 x0 = ep.X0[o], x1 = ep.X1[o];
-      double kx = ep.kx[m], ky = ep.ky[m];
+      const double2 x0 = in.a, x1 = in.c;
+      const double kx = in.s0, ky = in.s1;
       double re = (acc.x + (0.0 * x0.x - kx * x0.y)) + (0.0 * x1.x - ky * x1.y);
       double im = (acc.y + (0.0 * x0.y + kx * x0.x)) + (0.0 * x1.y + ky * x1.x);
       return make_double2(ep.s * re, ep.s * im);
     }
     case EPI_LAPRHS: {
-      const size_t oh = (size_t)b * ep.sH + (size_t)r * ep.M + m;
-      const size_t ou = (size_t)b * ep.sU + (size_t)r * ep.M + m;
-      double2 h = ep.H[oh], u = ep.U[ou];
-      double dx2 = ep.dx2[m], dy2 = ep.dy2[m];
+      const double2 h = in.a, u = in.c;
+      const double dx2 = in.s0, dy2 = in.s1;
       double lre = (acc.x + dx2 * u.x) + dy2 * u.x;
       double lim = (acc.y + dx2 * u.y) + dy2 * u.y;
       double ac2 = ep.a * ep.c2;
       return make_double2((ac2 * h.x + ep.a * u.x) - lre, (ac2 * h.y + ep.a * u.y) - lim);
     }
     case EPI_GRAD: {
-      const size_t o = (size_t)b * ep.sX + (size_t)r * ep.M + m;
+      const double2 x = in.a;
+      const double kx = in.s0, ky = in.s1;
       const size_t oa = (size_t)b * ep.sAux + (size_t)r * ep.M + m;
-      double2 x = ep.X0[o];
-      double kx = ep.kx[m], ky = ep.ky[m];
       ep.aux0[oa] = make_double2(0.0 * x.x - kx * x.y, 0.0 * x.y + kx * x.x);
       ep.aux1[oa] = make_double2(0.0 * x.x - ky * x.y, 0.0 * x.y + ky * x.x);
       return acc;
@@ -116,6 +156,70 @@ struct GemmArgs {
 };
 
 constexpr int kMaxGroup = 3;
+
+// output of a dense tile through the epilogue MODE, one m-tile at a time
+template <int MT, int MODE>
+__device__ __forceinline__ void dense_store(const GemmArgs& g, int b, int r0, int j0, const double (&acc)[MT][2][2]) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double2* Cb = reinterpret_cast<double2*>(g.C) + (size_t)b * g.out_stride;
+#pragma unroll
+  for (int mt = 0; mt < MT; ++mt) {
+    const int r = r0 + mt * 8 + (lane >> 2);
+    EpiIn in[2];
+    bool ok[2];
+    int m[2];
+#pragma unroll
+    for (int nt = 0; nt < 2; ++nt) {
+      m[nt] = (j0 + warp * 16 + nt * 8) / 2 + (lane & 3);
+      ok[nt] = r < g.rows && m[nt] < g.M;
+      if (ok[nt]) in[nt] = epi_load<MODE>(g.ep, b, r, m[nt]);
+    }
+#pragma unroll
+    for (int nt = 0; nt < 2; ++nt)
+      if (ok[nt])
+        Cb[(size_t)r * g.M + m[nt]] =
+            epi_apply<MODE>(g.ep, b, r, m[nt], make_double2(acc[mt][nt][0], acc[mt][nt][1]), in[nt]);
+  }
+}
+
+// output of a folded tile (rows i and n-1-i) through the epilogue MODE
+template <int MT, int MODE>
+__device__ __forceinline__ void sym_store(const GemmArgs& g, int b, int r0, int j0, const double (&accE)[MT][2][2],
+                                          const double (&accO)[MT][2][2]) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int n = g.nz, h = (g.nz - 1) / 2;
+  const double s = (double)g.sgn;
+  double2* Cb = reinterpret_cast<double2*>(g.C) + (size_t)b * g.out_stride;
+#pragma unroll
+  for (int mt = 0; mt < MT; ++mt) {
+    const int i = r0 + mt * 8 + (lane >> 2);
+    const int j = n - 1 - i;
+    bool ok[2];
+    int m[2];
+#pragma unroll
+    for (int nt = 0; nt < 2; ++nt) {
+      m[nt] = (j0 + warp * 16 + nt * 8) / 2 + (lane & 3);
+      ok[nt] = m[nt] < g.M;
+    }
+#pragma unroll
+    for (int half = 0; half < 2; ++half) {  // row i (P + Q), then row n-1-i (s (P - Q))
+      const int r = half == 0 ? i : j;
+      const bool row_ok = half == 0 ? i <= h : i < h;
+      EpiIn in[2];
+#pragma unroll
+      for (int nt = 0; nt < 2; ++nt)
+        if (row_ok && ok[nt]) in[nt] = epi_load<MODE>(g.ep, b, r, m[nt]);
+#pragma unroll
+      for (int nt = 0; nt < 2; ++nt) {
+        if (!(row_ok && ok[nt])) continue;
+        const double pe = accE[mt][nt][0], pi = accE[mt][nt][1], qe = accO[mt][nt][0], qi = accO[mt][nt][1];
+        const double2 v = half == 0 ? make_double2(pe + qe, pi + qi) : make_double2(s * (pe - qe), s * (pi - qi));
+        Cb[(size_t)r * g.M + m[nt]] = epi_apply<MODE>(g.ep, b, r, m[nt], v, in[nt]);
+      }
+    }
+  }
+}
+
 
 // ---------------------------------------------------------------------------
 // dense: out rows [r0, r0 + 8*MT), columns [j0, j0 + 128) reals
@@ -194,17 +298,12 @@ __device__ __forceinline__ void dense_body(const GemmArgs& g, const int b) {
     __syncthreads();
   }
 
-  double2* Cb = reinterpret_cast<double2*>(g.C) + (size_t)b * g.out_stride;
-#pragma unroll
-  for (int mt = 0; mt < MT; ++mt) {
-    const int r = r0 + mt * 8 + (lane >> 2);
-    if (r >= g.rows) continue;
-#pragma unroll
-    for (int nt = 0; nt < 2; ++nt) {
-      const int m = (j0 + warp * 16 + nt * 8) / 2 + (lane & 3);
-      if (m >= g.M) continue;
-      Cb[(size_t)r * g.M + m] = epilogue(g.ep, b, r, m, make_double2(acc[mt][nt][0], acc[mt][nt][1]));
-    }
+  switch (g.ep.mode) {
+    case EPI_RSCALE: dense_store<MT, EPI_RSCALE>(g, b, r0, j0, acc); break;
+    case EPI_DIV: dense_store<MT, EPI_DIV>(g, b, r0, j0, acc); break;
+    case EPI_LAPRHS: dense_store<MT, EPI_LAPRHS>(g, b, r0, j0, acc); break;
+    case EPI_GRAD: dense_store<MT, EPI_GRAD>(g, b, r0, j0, acc); break;
+    default: dense_store<MT, EPI_STORE>(g, b, r0, j0, acc); break;
   }
 }
 
@@ -302,23 +401,12 @@ __device__ __forceinline__ void sym_body(const GemmArgs& g, const int b) {
     __syncthreads();
   }
 
-  double2* Cb = reinterpret_cast<double2*>(g.C) + (size_t)b * g.out_stride;
-  const double s = (double)g.sgn;
-#pragma unroll
-  for (int mt = 0; mt < MT; ++mt) {
-    const int i = r0 + mt * 8 + (lane >> 2);
-    if (i > h) continue;
-#pragma unroll
-    for (int nt = 0; nt < 2; ++nt) {
-      const int m = (j0 + warp * 16 + nt * 8) / 2 + (lane & 3);
-      if (m >= g.M) continue;
-      const double pe = accE[mt][nt][0], pi = accE[mt][nt][1], qe = accO[mt][nt][0], qi = accO[mt][nt][1];
-      Cb[(size_t)i * g.M + m] = epilogue(g.ep, b, i, m, make_double2(pe + qe, pi + qi));
-      if (i < h) {
-        const int j = n - 1 - i;
-        Cb[(size_t)j * g.M + m] = epilogue(g.ep, b, j, m, make_double2(s * (pe - qe), s * (pi - qi)));
-      }
-    }
+  switch (g.ep.mode) {
+    case EPI_RSCALE: sym_store<MT, EPI_RSCALE>(g, b, r0, j0, accE, accO); break;
+    case EPI_DIV: sym_store<MT, EPI_DIV>(g, b, r0, j0, accE, accO); break;
+    case EPI_LAPRHS: sym_store<MT, EPI_LAPRHS>(g, b, r0, j0, accE, accO); break;
+    case EPI_GRAD: sym_store<MT, EPI_GRAD>(g, b, r0, j0, accE, accO); break;
+    default: sym_store<MT, EPI_STORE>(g, b, r0, j0, accE, accO); break;
   }
 }
 
