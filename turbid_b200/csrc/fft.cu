@@ -340,13 +340,22 @@ __global__ void __launch_bounds__(NB * L / 16) fx_p2_kernel(TransformDims d, con
   const int plane = blockIdx.y;
   const int y0 = blockIdx.x * rows;
   const T* src = phys + (size_t)plane * d.ny * L;
-#pragma unroll 4
-  for (int idx = threadIdx.x; idx < NB * L; idx += NT) {
-    const int p = idx / L, x = idx % L;
-    const int ya = y0 + 2 * p, yb = ya + 1;
-    const T re = ya < d.ny ? src[(size_t)ya * L + x] : T(0);
-    const T im = yb < d.ny ? src[(size_t)yb * L + x] : T(0);
-    buf[p * RS + sp(x)] = mkc<C>(re, im);
+  {
+    constexpr int IT = NB * L / NT;  // 16: every load of the tile in flight before the first shared store
+    T re[IT], im[IT];
+#pragma unroll
+    for (int i = 0; i < IT; ++i) {
+      const int idx = threadIdx.x + i * NT;
+      const int p = idx / L, x = idx % L;
+      const int ya = y0 + 2 * p, yb = ya + 1;
+      re[i] = ya < d.ny ? src[(size_t)ya * L + x] : T(0);
+      im[i] = yb < d.ny ? src[(size_t)yb * L + x] : T(0);
+    }
+#pragma unroll
+    for (int i = 0; i < IT; ++i) {
+      const int idx = threadIdx.x + i * NT;
+      buf[(idx / L) * RS + sp(idx % L)] = mkc<C>(re[i], im[i]);
+    }
   }
   __syncthreads();
   ip_passes<T, -1, L, NB, 1>(buf, tw);
@@ -381,10 +390,20 @@ __global__ void __launch_bounds__(NB * L / 16) fy_p2_kernel(TransformDims d, con
   const int plane = blockIdx.y;
   const int k0 = blockIdx.x * NB;
   const C* src = work + (size_t)plane * d.nxh * L;
-#pragma unroll 4
-  for (int idx = threadIdx.x; idx < NB * L; idx += NT) {
-    const int c = idx / L, y = idx % L;
-    buf[c * RS + sp(y)] = k0 + c < d.nxh ? src[(size_t)(k0 + c) * L + y] : mkc<C>(0, 0);
+  {
+    constexpr int IT = NB * L / NT;
+    C v[IT];
+#pragma unroll
+    for (int i = 0; i < IT; ++i) {
+      const int idx = threadIdx.x + i * NT;
+      const int c = idx / L, y = idx % L;
+      v[i] = k0 + c < d.nxh ? src[(size_t)(k0 + c) * L + y] : mkc<C>(0, 0);
+    }
+#pragma unroll
+    for (int i = 0; i < IT; ++i) {
+      const int idx = threadIdx.x + i * NT;
+      buf[(idx / L) * RS + sp(idx % L)] = v[i];
+    }
   }
   __syncthreads();
   ip_passes<T, -1, L, NB, 1>(buf, tw);
@@ -453,12 +472,20 @@ __global__ void __launch_bounds__(NB * L / 16) bx_p2_kernel(TransformDims d, con
   }
   const C* src = work + (size_t)plane * nxh * d.ny;
   const int total = rows * nxh;  // even; the pair (2p, 2p+1) sits in adjacent lanes
-  for (int base = 0; base < total; base += NT) {
-    const int idx = base + threadIdx.x;
+  constexpr int IT = (rows * (L / 3 + 1) + NT - 1) / NT;  // nxh <= L/3 + 1
+  C hv[IT];
+#pragma unroll
+  for (int i = 0; i < IT; ++i) {  // every load in flight before the pairs are combined
+    const int idx = threadIdx.x + i * NT;
+    const int k = idx / rows, q = idx % rows;
+    hv[i] = (idx < total && y0 + q < d.ny) ? src[(size_t)k * d.ny + y0 + q] : mkc<C>(0, 0);
+  }
+#pragma unroll
+  for (int i = 0; i < IT; ++i) {
+    const int idx = threadIdx.x + i * NT;
     const bool ok = idx < total;
     const int k = idx / rows, q = idx % rows;
-    const int y = y0 + q;
-    C h = (ok && y < d.ny) ? src[(size_t)k * d.ny + y] : mkc<C>(0, 0);
+    C h = hv[i];
     if (k == 0) h.y = T(0);
     C o;
     o.x = __shfl_xor_sync(0xffffffffu, h.x, 1);
