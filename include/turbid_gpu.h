@@ -138,7 +138,11 @@ TG_API tg_status tg_upload_state(tg_ctx* ctx, const double* uvw, const double* p
 TG_API tg_status tg_download_state(tg_ctx* ctx, double* uvw, double* p, double* phi);
 
 /* Time bookkeeping of TimeStepper (src/stepper_time.h:56-91): the phases read
- * time, dt, step and the alternation flag from here. */
+ * time, dt, step and the alternation flag from here.  A dt different from the
+ * current one (the adaptive branch, TimeStepper::Update2,
+ * src/stepper_time.cc:117-208) also re-assembles the velocity and scalar
+ * solves as FlatCarrierPhase::Update / FlatScalarPhase::Update do
+ * (src/phase_carrier_flat.cc:248-262, src/phase_scalar_flat.cc:225-238). */
 TG_API tg_status tg_set_time(tg_ctx* ctx, int step, double time, double dt, int alternation);
 TG_API tg_status tg_get_time(const tg_ctx* ctx, int* step, double* time, double* dt,
                       int* alternation, int* isforward, double* cfl);

@@ -240,6 +240,10 @@ inline std::string Upper(std::string s) {
 struct RunControl {
   int maxstep = 0, writeinterval = 1, startstep = 0, output_based_on_step = 1;
   double maxcfl = 1.0;
+  // adaptive-dt branch (output_based_on_step = 0), src/stepper_time.cc:31-37
+  double max_marching_time = 0, output_interval = 0, initial_time_step = 0;
+  int start_time_index = -1;
+  double cfl_adjust_scale[2] = {0.95, 0.9};
 };
 
 // The tg_case fields and run control from a configuration file (the keys of
@@ -278,6 +282,17 @@ inline tg_case CaseFromIni(const IniFile& ini, RunControl& rc, int precision = T
   rc.maxstep = ini.GetValueInt("Time Stepper", "maximum_task_step");
   rc.writeinterval = ini.GetValueInt("Time Stepper", "result_write_interval");
   rc.startstep = ini.GetValueInt("Time Stepper", "task_start_step");
+  if (rc.output_based_on_step == 0) {
+    rc.max_marching_time = ini.GetValueDouble("Time Stepper", "max_marching_time");
+    rc.output_interval = ini.GetValueDouble("Time Stepper", "output_interval");
+    rc.initial_time_step = ini.GetValueDouble("Time Stepper", "initial_time_step");
+    rc.start_time_index = ini.GetValueInt("Time Stepper", "task_start_time_index");
+    const std::vector<double> adj = ini.GetVectorDouble("Time Stepper", "cfl_adjust_scale");
+    if (adj.size() < 2) throw std::runtime_error("TimeStepper::Configuration::Load(IniFile) > cfl_adjust_scale needs 2 values");
+    rc.cfl_adjust_scale[0] = adj[0];
+    rc.cfl_adjust_scale[1] = adj[1];
+    c.dt = rc.initial_time_step;  // the solves are assembled for the first dt
+  }
   const std::string s = "Phase Carrier";
   const std::string ft = Upper(ini.GetValueString(s, "applied_force_type"));
   if (ft == "NONE") c.force_type = 0;
@@ -385,18 +400,26 @@ class GpuCase {
 
 // ---------------------------------------------------------------------------
 // RK3TimeStepper: coefficients live in the library; the host keeps the step,
-// time, CFL and the forward / output flags (TimeStepper::Update, fixed dt).
+// time, dt, CFL and the forward / output flags (TimeStepper::Configure,
+// Update for a fixed dt, Update2 for the adaptive dt).
 // ---------------------------------------------------------------------------
 class RK3TimeStepper {
  public:
+  // TimeStepper::Configure (src/stepper_time.cc:215-246)
   void Configure(const tg_case& c, const RunControl& rc) {
-    if (rc.output_based_on_step != 1)
-      throw std::runtime_error("RK3TimeStepper::Configure > Only output_based_on_step = 1 (fixed dt) is Supported!");
     rc_ = rc;
-    dt_ = c.dt;
-    step_ = std::max(0, rc.startstep);
-    time_ = step_ * dt_;
-    isforward_ = step_ < rc.maxstep;
+    if (rc.output_based_on_step) {
+      step_ = std::max(0, rc.startstep);
+      dt_ = c.dt;
+      time_ = step_ * dt_;
+      isforward_ = step_ <= rc.maxstep;
+    } else {
+      step_ = 0;
+      dt_ = rc.initial_time_step;
+      time_ = rc.start_time_index > 0 ? rc.start_time_index * rc.output_interval : 0.0;
+      output_time_index_ = rc.start_time_index;
+      isforward_ = time_ <= rc.max_marching_time;
+    }
   }
   // TimeStepper::Update (src/stepper_time.cc:72-113)
   void Update(double maxulen) {
@@ -411,12 +434,45 @@ class RK3TimeStepper {
       isoutput_ = true;
     }
   }
+  // TimeStepper::Update2 (src/stepper_time.cc:117-208): time advances by the
+  // previous dt, then dt is rescaled towards the CFL band and clipped to land
+  // on the next output time.
+  void Update2(double maxulen) {
+    if (!isforward_) return;
+    step_ += 1;
+    time_ = time_ + dt_;
+    isforward_ = time_ < rc_.max_marching_time;
+    cfl_ = maxulen * dt_;
+    if (cfl_ > 0) {
+      const double top = rc_.cfl_adjust_scale[0], bot = rc_.cfl_adjust_scale[1];
+      if (cfl_ > top * rc_.maxcfl) {
+        dt_ = dt_ * top;
+        while (maxulen * dt_ > top * rc_.maxcfl) dt_ = dt_ * top;
+      } else if (cfl_ < bot * rc_.maxcfl) {
+        dt_ = dt_ * 1.05;
+      }
+      if ((time_ + dt_) / rc_.output_interval - output_time_index_ - 1 >= 0) {
+        const double dttmp = (output_time_index_ + 1) * rc_.output_interval - time_;
+        dt_ = dttmp < rc_.initial_time_step / 100 ? dt_ / 20 : dttmp;
+        output_time_index_ = output_time_index_ + 1;
+        isoutput_ = true;
+      } else {
+        isoutput_ = false;
+      }
+    }
+    if (cfl_ > rc_.maxcfl * 1.1 || dt_ < rc_.initial_time_step / 1000) {
+      isforward_ = false;
+      isoutput_ = true;
+    }
+  }
   void SetAlternationFlag() { alternation_ = !alternation_; }
   bool isForward() const { return isforward_; }
   bool isOutput() const { return isoutput_; }
-  bool isOutputOnStep() const { return rc_.output_based_on_step == 1; }
+  bool isOutputOnStep() const { return rc_.output_based_on_step != 0; }
   bool GetAlternationFlag() const { return alternation_; }
   int GetStep() const { return step_; }
+  int GetOutputTimeIndex() const { return output_time_index_; }
+  int GetStartIndex() const { return isOutputOnStep() ? rc_.startstep : rc_.start_time_index; }
   double GetTime() const { return time_; }
   double GetCfl() const { return cfl_; }
   double GetTimeStep() const { return dt_; }
@@ -424,7 +480,7 @@ class RK3TimeStepper {
  private:
   RunControl rc_;
   double dt_ = 0, time_ = 0, cfl_ = 0;
-  int step_ = 0;
+  int step_ = 0, output_time_index_ = 0;
   bool isforward_ = false, isoutput_ = false, alternation_ = false;
 };
 
@@ -540,7 +596,10 @@ class FlatChannelSolver {
     if (c.nphase > 1) scalar_.reset(new FlatScalarPhase(*gpu_));
     variables_.reset(new FlatVariables(*gpu_));
     tstepper_.Configure(c, rc_);
-    variables_->Load(directory_ + std::to_string((long long)std::max(0, rc_.startstep)) + "/", tstepper_.GetStep());
+    // FlatCarrierVariable::Configure (src/variable_carrier_flat.cc:386-401)
+    const int inputindex = tstepper_.GetStartIndex();
+    if (inputindex < 0) throw std::runtime_error("FlatCarrierVariable::Configure > A Restart State is Required (start index < 0)");
+    variables_->Load(directory_ + std::to_string((long long)inputindex) + "/", tstepper_.GetStep());
     configured_ = true;
   }
   bool isConfigured() const { return configured_; }
@@ -553,8 +612,13 @@ class FlatChannelSolver {
     std::vector<double> feature = carrier_->GetFeatureGlobal();
     while (tstepper_.isForward()) {
       // a CFL above the limit (or the last step) clears the forward flag; the
-      // step is still taken and, with the output flag, written for record
-      tstepper_.Update(feature[19]);
+      // step is still taken and, with the output flag, written for record.
+      // With the adaptive dt, tg_set_time re-assembles the solves for the new
+      // dt (FlatCarrierPhase::Update / FlatScalarPhase::Update).
+      if (tstepper_.isOutputOnStep())
+        tstepper_.Update(feature[19]);
+      else
+        tstepper_.Update2(feature[19]);
       Check("TimeStepper::Update", tg_set_time(gpu_->ctx(), tstepper_.GetStep(), tstepper_.GetTime(),
                                                 tstepper_.GetTimeStep(), tstepper_.GetAlternationFlag() ? 1 : 0));
       for (int stage = 0; stage < 3; ++stage) {
@@ -567,8 +631,10 @@ class FlatChannelSolver {
       }
       tstepper_.SetAlternationFlag();
       feature = carrier_->GetFeatureGlobal();
-      if (tstepper_.isOutput())
-        variables_->Save(directory_ + std::to_string((long long)tstepper_.GetStep()) + "/");
+      if (tstepper_.isOutput()) {
+        const int index = tstepper_.isOutputOnStep() ? tstepper_.GetStep() : tstepper_.GetOutputTimeIndex();
+        variables_->Save(directory_ + std::to_string((long long)index) + "/");
+      }
       std::ostringstream line;
       PrintLogBody(line, feature);
       std::cout << line.str();

@@ -186,6 +186,12 @@ class CaseConfig:
     erosion_rate: float = 0.0
     critical_shear: float = 0.0
     scalar_bc: int = 1   # 0 ZeroFlux, 1 ErosionDeposition (src/phase_scalar_flat.h:23-26)
+    # adaptive-dt branch (output_based_on_step = 0), src/stepper_time.cc:31-37
+    max_marching_time: float = 1e300
+    output_interval: float = 1e300
+    initial_time_step: float = 0.0
+    start_time_index: int = -1
+    cfl_adjust_scale: List[float] = field(default_factory=lambda: [0.95, 0.9])
 
     @classmethod
     def from_ini(cls, ini: IniFile) -> "CaseConfig":
@@ -205,6 +211,12 @@ class CaseConfig:
         c.writeinterval = ini.int("Time Stepper", "result_write_interval")
         c.dt = ini.double("Time Stepper", "marching_time_step")
         c.startstep = ini.int("Time Stepper", "task_start_step")
+        if c.output_based_on_step == 0:
+            c.max_marching_time = ini.double("Time Stepper", "max_marching_time")
+            c.output_interval = ini.double("Time Stepper", "output_interval")
+            c.initial_time_step = ini.double("Time Stepper", "initial_time_step")
+            c.start_time_index = ini.int("Time Stepper", "task_start_time_index")
+            c.cfl_adjust_scale = ini.vec("Time Stepper", "cfl_adjust_scale")
         s = "Phase Carrier"
         c.force_type = FORCE_TYPES[ini.string(s, "applied_force_type").upper()]
         c.force_direction = [int(v) for v in ini.vec(s, "force_direction")]
@@ -569,11 +581,19 @@ class OracleSolver:
         g = self.g = Grid(cfg)
         self.D1, self.D2 = chebyshev_d1_d2(g, cfg.mapping, cfg.mapping_coef)
         n = g.nz
-        # --- TimeStepper::Configure (src/stepper_time.cc:215-246), fixed-dt branch
-        self.step = max(0, cfg.startstep)
-        self.dt = cfg.dt
-        self.time = self.step * self.dt
-        self.isforward = self.step <= cfg.maxstep
+        # --- TimeStepper::Configure (src/stepper_time.cc:215-246)
+        self.output_time_index = 0
+        if cfg.output_based_on_step:
+            self.step = max(0, cfg.startstep)
+            self.dt = cfg.dt
+            self.time = self.step * self.dt
+            self.isforward = self.step <= cfg.maxstep
+        else:
+            self.step = 0
+            self.dt = cfg.initial_time_step
+            self.time = cfg.start_time_index * cfg.output_interval if cfg.start_time_index > 0 else 0.0
+            self.output_time_index = cfg.start_time_index
+            self.isforward = self.time <= cfg.max_marching_time
         self.isoutput = False
         self.cfl = 0.0
         self.alternation = False
@@ -906,8 +926,57 @@ class OracleSolver:
             self.isforward = False
             self.isoutput = True
 
+    def time_update2(self):
+        """TimeStepper::Update2 (src/stepper_time.cc:117-208): the adaptive-dt
+        branch.  time advances by the previous dt, then dt is rescaled towards
+        the CFL band and clipped to land on the next output time."""
+        cfg = self.cfg
+        if not self.isforward:
+            return
+        maxulen = self.fglobal[19]
+        self.step += 1
+        self.time = self.time + self.dt
+        self.isforward = self.time < cfg.max_marching_time
+        self.cfl = maxulen * self.dt
+        if self.cfl > 0:
+            top, bot = cfg.cfl_adjust_scale[0], cfg.cfl_adjust_scale[1]
+            if self.cfl > top * cfg.maxcfl:
+                self.dt = self.dt * top
+                while maxulen * self.dt > top * cfg.maxcfl:
+                    self.dt = self.dt * top
+            elif self.cfl < bot * cfg.maxcfl:
+                self.dt = self.dt * 1.05
+            if (self.time + self.dt) / cfg.output_interval - self.output_time_index - 1 >= 0:
+                dttmp = (self.output_time_index + 1) * cfg.output_interval - self.time
+                if dttmp < cfg.initial_time_step / 100:
+                    self.dt = self.dt / 20
+                else:
+                    self.dt = dttmp
+                self.output_time_index += 1
+                self.isoutput = True
+            else:
+                self.isoutput = False
+        if self.cfl > cfg.maxcfl * 1.1 or self.dt < cfg.initial_time_step / 1000:
+            self.isforward = False
+            self.isoutput = True
+
+    def phase_update(self):
+        """FlatCarrierPhase::Update / FlatScalarPhase::Update
+        (src/phase_carrier_flat.cc:248-262, src/phase_scalar_flat.cc:225-238):
+        the reciprocals re-assembled for the current dt (pressure unchanged)."""
+        cfg, g = self.cfg, self.g
+        sc = [-cfg.reynolds / self.dt / RK3[2, s] for s in range(3)]
+        for d in (self.dec_u, self.dec_v, self.dec_w):
+            d.assemble(g, sc)
+        if self.scalar:
+            self.dec_s.assemble(g, [-cfg.reynolds * cfg.schmidt / self.dt / RK3[2, s] for s in range(3)])
+
     def run_step(self):
-        self.time_update()
+        if self.cfg.output_based_on_step:
+            self.time_update()
+        else:
+            self.time_update2()
+            self.phase_update()
         for stage in range(3):
             self.carrier_predict(stage)
             self.carrier_correct(stage)

@@ -40,8 +40,11 @@ def write_ini(path, cfg: O.CaseConfig, maxstep: int, writeinterval: int, startst
         "[Space Stepper]", "applied_stepper_type = Chebyshev", f"mapping_function = {mapping}",
         f"mapping_coefficient = {cfg.mapping_coef!r} 0",
         "[Time Stepper]", "applied_stepper_type = RungeKutta3", f"marching_time_step = {dt_expr or repr(cfg.dt)}",
-        "output_based_on_step = 1", f"maximum_cfl_number = {cfg.maxcfl!r}", f"maximum_task_step = {maxstep}",
-        f"result_write_interval = {writeinterval}", f"task_start_step = {startstep}",
+        f"output_based_on_step = {cfg.output_based_on_step}", f"maximum_cfl_number = {cfg.maxcfl!r}",
+        f"maximum_task_step = {maxstep}", f"result_write_interval = {writeinterval}", f"task_start_step = {startstep}",
+        f"max_marching_time = {cfg.max_marching_time!r}", f"output_interval = {cfg.output_interval!r}",
+        f"initial_time_step = {cfg.initial_time_step!r}", f"task_start_time_index = {cfg.start_time_index}",
+        f"cfl_adjust_scale = {_fmt(cfg.cfl_adjust_scale)}", "result_write_initial = 0",
         "[Phase Carrier]", f"applied_force_type = {force}", f"force_direction = {cfg.force_direction[0]} {cfg.force_direction[1]}",
         f"force_amplitude = {_fmt(cfg.force_amplitude)}", f"reynolds_number = {cfg.reynolds!r}",
         f"froude_number = {cfg.froude!r}", f"averaged_concentration = {cfg.averaged_concentration!r}",
@@ -90,6 +93,58 @@ def test_driver_parses_like_python(driver, tmp_path):
     assert got["maxstep"] == 7 and got["writeinterval"] == 7 and got["startstep"] == 0
 
 
+def adaptive_cfg(**kw):
+    dt0 = 2 * math.pi / 2000
+    base = dict(output_based_on_step=0, initial_time_step=dt0, output_interval=2.5 * dt0,
+                max_marching_time=4.2 * dt0, start_time_index=0, cfl_adjust_scale=[0.95, 0.9], maxcfl=0.05)
+    base.update(kw)
+    return sediment_cfg(**base)
+
+
+def test_driver_parses_adaptive_keys(driver, tmp_path):
+    cfg = adaptive_cfg()
+    ini = tmp_path / "configuration.ini"
+    write_ini(ini, cfg, maxstep=7, writeinterval=7)
+    got = json.loads(subprocess.run([driver, "--parse-only", str(ini)], capture_output=True, text=True,
+                                    check=True).stdout)
+    ref = tconfig.params_from_ini(tconfig.Ini.load(str(ini)))
+    for k in ("max_marching_time", "output_interval", "initial_time_step", "start_time_index", "dt"):
+        assert got[k] == ref[k], k
+    assert got["cfl_adjust_scale"] == ref["cfl_adjust_scale"] and got["dt"] == cfg.initial_time_step
+
+
+@pytest.mark.parametrize("adaptive", [False, True])
+def test_time_stepper_matches_oracle(driver, tmp_path, adaptive):
+    """TimeStepper::Update / Update2 of the C++ layer against the oracle on a
+    sequence of maximum velocity/length values (no GPU)."""
+    cfg = adaptive_cfg() if adaptive else sediment_cfg(maxcfl=0.2)
+    cfg.maxstep, cfg.writeinterval = 9, 3
+    ini = tmp_path / "configuration.ini"
+    write_ini(ini, cfg, maxstep=cfg.maxstep, writeinterval=cfg.writeinterval)
+    lens = [0.0, 12.0, 30.0, 31.0, 8.0, 2.0, 55.0, 70.0, 40.0, 5.0, 5.0, 5.0]
+    out = subprocess.run([driver, "--time-only", str(ini)] + [repr(v) for v in lens], capture_output=True,
+                         text=True, check=True).stdout
+    got = [json.loads(l) for l in out.strip().splitlines()]
+    uvw, p, phi = O.make_initial_state(cfg, seed=3, noise=0.01)
+    sol = O.OracleSolver(cfg, uvw, p, phi)
+    ref = []
+    for v in lens:
+        if not sol.isforward:
+            break
+        sol.fglobal[19] = v
+        sol.time_update() if not adaptive else sol.time_update2()
+        ref.append(dict(step=sol.step, time=sol.time, dt=sol.dt, cfl=sol.cfl, forward=int(sol.isforward),
+                        output=int(sol.isoutput), output_index=sol.output_time_index))
+    assert len(got) == len(ref) and len(ref) >= 3
+    for a, b in zip(got, ref):
+        for k in ("step", "forward", "output", "output_index"):
+            assert a[k] == b[k], (k, a, b)
+        for k in ("time", "dt", "cfl"):
+            assert a[k] == pytest.approx(b[k], rel=1e-15, abs=1e-300), (k, a, b)
+    if adaptive:
+        assert len({round(r["dt"], 12) for r in ref}) > 2   # dt did change
+
+
 def test_driver_rejects_bad_config(driver, tmp_path):
     cfg = sediment_cfg()
     ini = tmp_path / "configuration.ini"
@@ -111,6 +166,35 @@ def test_expression_evaluator_matches_python(driver, tmp_path):
         write_ini(ini, cfg, maxstep=1, writeinterval=1, dt_expr=ex)
         out = subprocess.run([driver, "--parse-only", str(ini)], capture_output=True, text=True, check=True).stdout
         assert json.loads(out)["dt"] == pytest.approx(tconfig.expression(ex), rel=1e-15, abs=1e-300), ex
+
+
+@pytest.mark.gpu
+def test_driver_adaptive_dt(cuda, driver, tmp_path):
+    """output_based_on_step = 0: dt follows the CFL band and lands on the output
+    time; the solves are re-assembled for each dt.  The restart files of output
+    time index 1 match the oracle's state at its first output."""
+    cfg = adaptive_cfg()
+    uvw, p, phi = O.make_initial_state(cfg, seed=22, noise=0.05)
+    write_ini(tmp_path / "configuration.ini", cfg, maxstep=100, writeinterval=100)
+    O.write_phase_file(str(tmp_path / "0" / "phase_00_variable.dat"), [uvw, p])
+    O.write_phase_file(str(tmp_path / "0" / "phase_01_variable.dat"), [phi])
+    r = subprocess.run([driver, str(tmp_path / "configuration.ini")], capture_output=True, text=True,
+                       cwd=str(tmp_path), timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    sol = O.OracleSolver(cfg, uvw, p, phi)
+    first = None
+    dts = []
+    while sol.isforward:
+        sol.run_step()
+        dts.append(sol.dt)
+        if sol.isoutput and first is None:
+            first = (sol.output_time_index, sol.uvw.copy(), sol.p.copy(), sol.phi.copy())
+    assert first is not None and first[0] == 1 and len(set(dts)) > 1
+    nlines = len(r.stdout.strip().splitlines())
+    assert nlines == len(dts)
+    gu, gp = O.read_phase_file(str(tmp_path / "1" / "phase_00_variable.dat"), [3, 1])
+    (gc,) = O.read_phase_file(str(tmp_path / "1" / "phase_01_variable.dat"), [1])
+    assert O.rel_l2(gu, first[1]) < 1e-9 and O.rel_l2(gp, first[2]) < 1e-9 and O.rel_l2(gc, first[3]) < 1e-9
 
 
 @pytest.mark.gpu

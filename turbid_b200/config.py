@@ -116,6 +116,13 @@ def params_from_ini(ini: Ini) -> dict:
     p["maxstep"] = ini.i("Time Stepper", "maximum_task_step")
     p["writeinterval"] = ini.i("Time Stepper", "result_write_interval")
     p["startstep"] = ini.i("Time Stepper", "task_start_step")
+    if p["output_based_on_step"] == 0:  # adaptive dt (TimeStepper::Update2)
+        p["max_marching_time"] = ini.d("Time Stepper", "max_marching_time")
+        p["output_interval"] = ini.d("Time Stepper", "output_interval")
+        p["initial_time_step"] = ini.d("Time Stepper", "initial_time_step")
+        p["start_time_index"] = ini.i("Time Stepper", "task_start_time_index")
+        p["cfl_adjust_scale"] = ini.v("Time Stepper", "cfl_adjust_scale")
+        p["dt"] = p["initial_time_step"]
     s = "Phase Carrier"
     ft = ini.s(s, "applied_force_type").upper()
     if ft not in FORCES:

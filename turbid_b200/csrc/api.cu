@@ -950,9 +950,18 @@ tg_status tg_download_state(tg_ctx* ctx, double* uvw, double* p, double* phi) {
 tg_status tg_set_time(tg_ctx* ctx, int step, double time, double dt, int alternation) {
   TG_CHECK_CTX(ctx);
   Ctx& x = *reinterpret_cast<Ctx*>(ctx);
-  if (dt != x.dt) {
-    set_error("tg_set_time > dt differs from the assembled decompositions (adaptive dt is not supported)");
+  if (!(dt > 0.0)) {
+    set_error("TimeStepper::Update > dt must be positive");
     return TG_ERR_ARG;
+  }
+  if (dt != x.dt) {
+    // FlatCarrierPhase::Update / FlatScalarPhase::Update: the reciprocals of
+    // the velocity and scalar solves follow dt (the GEMM epilogue forms them
+    // from sigma); the pressure solve does not depend on dt
+    x.dt = dt;
+    for (int s = 0; s < 3; ++s) x.sig_u[s] = -x.c.reynolds / dt / RK3[2][s];
+    if (x.scalar)
+      for (int s = 0; s < 3; ++s) x.sig_s[s] = -x.c.reynolds * x.c.schmidt / dt / RK3[2][s];
   }
   x.step = step;
   x.time = time;

@@ -5,6 +5,9 @@
 //
 //   channelflat_gpu [configuration.ini [logcomputation]] [--mixed]
 //   channelflat_gpu --parse-only configuration.ini    (case parameters as JSON, no GPU)
+//   channelflat_gpu --time-only configuration.ini L1 L2 ...
+//       (the time stepper alone for the given per-step maximum velocity/length
+//        values: one JSON line per step with step, time, dt, cfl, flags; no GPU)
 #include <iostream>
 #include <string>
 
@@ -33,7 +36,10 @@ void PrintCaseJson(const tg_case& c, const turbid::RunControl& rc) {
     << ", \"schmidt\": " << c.schmidt << ", \"settling\": " << c.settling << ", \"erosion_rate\": " << c.erosion_rate
     << ", \"critical_shear\": " << c.critical_shear << ", \"scalar_bc\": " << c.scalar_bc
     << ", \"maxcfl\": " << rc.maxcfl << ", \"maxstep\": " << rc.maxstep << ", \"writeinterval\": " << rc.writeinterval
-    << ", \"startstep\": " << rc.startstep << "}";
+    << ", \"startstep\": " << rc.startstep << ", \"max_marching_time\": " << rc.max_marching_time
+    << ", \"output_interval\": " << rc.output_interval << ", \"initial_time_step\": " << rc.initial_time_step
+    << ", \"start_time_index\": " << rc.start_time_index << ", \"cfl_adjust_scale\": "
+    << vec(rc.cfl_adjust_scale, 2) << "}";
   std::cout << s.str() << std::endl;
 }
 }  // namespace
@@ -45,6 +51,24 @@ int main(int argc, char** argv) {
       ini.Load(argv[2]);
       turbid::RunControl rc;
       PrintCaseJson(turbid::CaseFromIni(ini, rc), rc);
+      return 0;
+    }
+    if (argc > 2 && std::string(argv[1]) == "--time-only") {
+      turbid::IniFile ini;
+      ini.Load(argv[2]);
+      turbid::RunControl rc;
+      const tg_case c = turbid::CaseFromIni(ini, rc);
+      turbid::RK3TimeStepper ts;
+      ts.Configure(c, rc);
+      for (int i = 3; i < argc && ts.isForward(); ++i) {
+        const double maxulen = std::atof(argv[i]);
+        if (ts.isOutputOnStep()) ts.Update(maxulen);
+        else ts.Update2(maxulen);
+        std::cout << std::setprecision(17) << "{\"step\": " << ts.GetStep() << ", \"time\": " << ts.GetTime()
+                  << ", \"dt\": " << ts.GetTimeStep() << ", \"cfl\": " << ts.GetCfl()
+                  << ", \"forward\": " << (ts.isForward() ? 1 : 0) << ", \"output\": " << (ts.isOutput() ? 1 : 0)
+                  << ", \"output_index\": " << ts.GetOutputTimeIndex() << "}" << std::endl;
+      }
       return 0;
     }
     turbid::FlatChannelSolver solver(argc, argv);
