@@ -162,6 +162,13 @@ TG_API tg_status tg_scalar_correct(tg_ctx* ctx, int stage);   /* phase_scalar_fl
  * 50-entry feature vector after the last step (one 400-byte device->host read). */
 TG_API tg_status tg_run_steps(tg_ctx* ctx, int nsteps, int maxstep, double maxcfl,
                        double* features, int* done);
+/* tg_run_steps records each of the two step variants (the nonlinear forms
+ * alternate) once as a CUDA graph and replays it when the step's kernel
+ * arguments do not change from step to step (fixed dt, flat bed, no profiling,
+ * a stream other than the legacy default stream); enable = 0 issues every
+ * kernel separately.  Results are identical either way.  Default: enabled.
+ * (No reference counterpart; execution control.) */
+TG_API tg_status tg_set_graphs(tg_ctx* ctx, int enable);
 
 /* Phase::GetFeatureGlobal (src/phase.h:57): 50 doubles, device -> host. */
 TG_API tg_status tg_features(tg_ctx* ctx, double* out);

@@ -102,6 +102,15 @@ struct Ctx {
   unsigned long long* bits = nullptr;
   double* feat_h = nullptr;   // pinned [2][100]
   cudaEvent_t fev[2] = {nullptr, nullptr};
+  // whole RK3 steps replayed as CUDA graphs (one per alternation parity): the
+  // only per-step kernel argument, the mean-mode forcing, goes through
+  // force_d, copied from the pinned slot force_h[parity] by the graph itself
+  bool graphs = true, capturing = false;
+  cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+  long long gkernels[2] = {0, 0};
+  cudaStream_t cap_s = nullptr;
+  double* force_d = nullptr;  // device [2]
+  double* force_h = nullptr;  // pinned [2 parities][2]
   std::vector<void*> allocs;
   Profiler prof;
   // time / phase state
@@ -121,9 +130,18 @@ struct Ctx {
     TG_CUDA(cudaMemset(p, 0, n * sizeof(X)));
     return reinterpret_cast<X*>(p);
   }
+  void drop_graphs() {
+    for (auto& g : gexec) {
+      if (g) cudaGraphExecDestroy(g);
+      g = nullptr;
+    }
+  }
   ~Ctx() {
+    drop_graphs();
+    if (cap_s) cudaStreamDestroy(cap_s);
     for (void* p : allocs) cudaFree(p);
     if (feat_h) cudaFreeHost(feat_h);
+    if (force_h) cudaFreeHost(force_h);
     for (auto& e : fev)
       if (e) cudaEventDestroy(e);
     fft_plan_destroy(px);
@@ -313,6 +331,9 @@ static Ctx* create(const tg_case& c) {
   x.bits = x.dalloc<unsigned long long>(16);
   TG_CUDA(cudaMallocHost(&x.feat_h, 2 * 100 * sizeof(double)));
   std::memset(x.feat_h, 0, 2 * 100 * sizeof(double));
+  x.force_d = x.dalloc<double>(2);
+  TG_CUDA(cudaMallocHost(&x.force_h, 4 * sizeof(double)));
+  std::memset(x.force_h, 0, 4 * sizeof(double));
   TG_CUDA(cudaEventCreateWithFlags(&x.fev[0], cudaEventDisableTiming));
   TG_CUDA(cudaEventCreateWithFlags(&x.fev[1], cudaEventDisableTiming));
   return px.release();
@@ -451,7 +472,7 @@ static void carrier_predict(Ctx& x, int stage) {
   double f1, f2;
   mean_force(x, f1, f2);
   h_update(x.H, x.ADV, phi, S, x.M, c1, dt, bcoef, std::sin(x.c.slope), std::cos(x.c.slope), x.c.slope_direction,
-           dt * f1, dt * f2, x.s);
+           dt * f1, dt * f2, x.capturing ? x.force_d : nullptr, x.s);
   // Laplacian and rhs (phase_carrier_flat.cc:517-536)
   {
     const double redtc3 = -x.c.reynolds / dt / c3;
@@ -723,6 +744,71 @@ static void download_state(Ctx& x, double* uvw, double* p, double* phi) {
 
 // FlatChannelSolver::Execute loop body; the CFL guard of TimeStepper::Update
 // for step n+1 uses the features of step n, read back while step n+1 runs.
+// A whole step can be replayed from a graph when none of its kernel arguments
+// changes from step to step except the forcing: a fixed dt (changing dt drops
+// the graphs), no sloped bed (its flux features run every tenth step only),
+// no active profiler, and a stream other than the legacy default stream.
+static bool graph_eligible(const Ctx& x) {
+  return x.graphs && x.c.slope_direction == 0 && !g_prof && x.s != nullptr;
+}
+
+template <typename T>
+static void record_step(Ctx& x) {
+  for (int st = 0; st < 3; ++st) run_stage<T>(x, st);
+}
+
+static void run_step_graph(Ctx& x) {
+  const int par = x.alternation ? 1 : 0;
+  double f1, f2;
+  mean_force(x, f1, f2);  // the same forcing for the three stages
+  // this pinned slot was last read two steps ago, which has completed
+  x.force_h[2 * par] = x.dt * f1;
+  x.force_h[2 * par + 1] = x.dt * f2;
+  if (!x.gexec[par]) {
+    if (!x.cap_s) TG_CUDA(cudaStreamCreateWithFlags(&x.cap_s, cudaStreamNonBlocking));
+    cudaStream_t user = x.s;
+    x.s = x.cap_s;
+    x.capturing = true;
+    cudaGraph_t g = nullptr;
+    try {
+      TG_CUDA(cudaStreamBeginCapture(x.s, cudaStreamCaptureModeThreadLocal));
+      TG_CUDA(cudaMemcpyAsync(x.force_d, x.force_h + 2 * par, 2 * sizeof(double), cudaMemcpyHostToDevice, x.s));
+      if (x.mixed)
+        record_step<float>(x);
+      else
+        record_step<double>(x);
+      TG_CUDA(cudaStreamEndCapture(x.s, &g));
+    } catch (...) {
+      cudaGraph_t dead = nullptr;
+      cudaStreamEndCapture(x.s, &dead);
+      if (dead) cudaGraphDestroy(dead);
+      x.s = user;
+      x.capturing = false;
+      throw;
+    }
+    x.s = user;
+    x.capturing = false;
+    size_t nn = 0;
+    TG_CUDA(cudaGraphGetNodes(g, nullptr, &nn));
+    std::vector<cudaGraphNode_t> nodes(nn);
+    TG_CUDA(cudaGraphGetNodes(g, nodes.data(), &nn));
+    long long kernels = 0;
+    for (auto nd : nodes) {
+      cudaGraphNodeType t;
+      TG_CUDA(cudaGraphNodeGetType(nd, &t));
+      if (t == cudaGraphNodeTypeKernel) ++kernels;
+    }
+    const cudaError_t e = cudaGraphInstantiate(&x.gexec[par], g, 0);
+    cudaGraphDestroy(g);
+    TG_CUDA(e);
+    x.gkernels[par] = kernels;
+    // the kernels recorded during capture were counted; they run with the launch below
+    g_launches -= kernels;
+  }
+  TG_CUDA(cudaGraphLaunch(x.gexec[par], x.s));
+  g_launches += x.gkernels[par];
+}
+
 static int run_steps(Ctx& x, int nsteps, int maxstep, double maxcfl, double* feat_out) {
   if (!x.loaded) throw Error{TG_ERR_STATE, "FlatChannelSolver::Execute > state not loaded"};
   int done = 0;
@@ -734,11 +820,12 @@ static int run_steps(Ctx& x, int nsteps, int maxstep, double maxcfl, double* fea
     x.step += 1;
     x.time = x.time + x.dt;
     bool fwd_flag = x.step < maxstep;
-    if (x.mixed) {
+    if (graph_eligible(x))
+      run_step_graph(x);
+    else if (x.mixed)
       for (int st = 0; st < 3; ++st) run_stage<float>(x, st);
-    } else {
+    else
       for (int st = 0; st < 3; ++st) run_stage<double>(x, st);
-    }
     x.alternation = !x.alternation;
     const int slot = done & 1;
     TG_CUDA(cudaMemcpyAsync(x.feat_h + slot * 100, x.feat, 100 * sizeof(double), cudaMemcpyDeviceToHost, x.s));
@@ -955,6 +1042,7 @@ tg_status tg_set_time(tg_ctx* ctx, int step, double time, double dt, int alterna
     return TG_ERR_ARG;
   }
   if (dt != x.dt) {
+    x.drop_graphs();  // dt is an argument of the recorded kernels
     // FlatCarrierPhase::Update / FlatScalarPhase::Update: the reciprocals of
     // the velocity and scalar solves follow dt (the GEMM epilogue forms them
     // from sigma); the pressure solve does not depend on dt
@@ -1013,6 +1101,14 @@ tg_status tg_scalar_predict(tg_ctx* ctx, int stage) {
 tg_status tg_scalar_correct(tg_ctx* ctx, int stage) {
   if (ctx && !has_scalar(ctx)) return TG_ERR_STATE;
   TG_STAGE_CALL(scalar_correct<float>(x, stage), scalar_correct<double>(x, stage));
+}
+
+tg_status tg_set_graphs(tg_ctx* ctx, int enable) {
+  TG_CHECK_CTX(ctx);
+  Ctx& x = *reinterpret_cast<Ctx*>(ctx);
+  x.graphs = enable != 0;
+  if (!x.graphs) x.drop_graphs();
+  return TG_OK;
 }
 
 tg_status tg_run_steps(tg_ctx* ctx, int nsteps, int maxstep, double maxcfl, double* features, int* done) {

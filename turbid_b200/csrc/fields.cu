@@ -146,8 +146,12 @@ void mul_shift(const T* a, const T* b, T* out, size_t P, double sh, cudaStream_t
 // --- carrier H register (phase_carrier_flat.cc:293-296, 325-356, 503-504) -------
 __global__ void k_h_update(double2* __restrict__ H, const double2* __restrict__ adv, const double2* __restrict__ phi,
                            size_t S, int M, double c1, double dt, double bcoef, double sinsl, double cossl, int sdir,
-                           double dtf1, double dtf2) {
+                           double dtf1, double dtf2, const double* __restrict__ dtf) {
   const size_t n = 3 * S;
+  if (dtf) {  // forcing of this step from device memory (graph replay)
+    dtf1 = dtf[0];
+    dtf2 = dtf[1];
+  }
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
     const int c = (int)(i / S);
     const size_t e = i - (size_t)c * S;
@@ -173,9 +177,10 @@ __global__ void k_h_update(double2* __restrict__ H, const double2* __restrict__ 
   }
 }
 void h_update(double2* H, const double2* adv, const double2* phi, size_t S, int M, double c1, double dt,
-              double bcoef, double sinsl, double cossl, int sdir, double dtf1, double dtf2, cudaStream_t s) {
+              double bcoef, double sinsl, double cossl, int sdir, double dtf1, double dtf2, const double* dtf,
+              cudaStream_t s) {
   prof_begin(s, PC_ELEM, 144.0 * (double)S, 0);
-  k_h_update<<<nblk(3 * S), kT, 0, s>>>(H, adv, phi, S, M, c1, dt, bcoef, sinsl, cossl, sdir, dtf1, dtf2);
+  k_h_update<<<nblk(3 * S), kT, 0, s>>>(H, adv, phi, S, M, c1, dt, bcoef, sinsl, cossl, sdir, dtf1, dtf2, dtf);
   prof_end(s);
   TG_LAUNCH_CHECK("k_h_update");
 }

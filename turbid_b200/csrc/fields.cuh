@@ -15,8 +15,10 @@ template <typename T>
 void phi_products(const T* phip, const T* unl, T* out, size_t P, double su, double sv, double sw, cudaStream_t s);
 template <typename T> void mul_shift(const T* a, const T* b, T* out, size_t P, double sh, cudaStream_t s);
 
+// dtf: when not null, the forcing pair (dt*f1, dt*f2) is read from device memory
 void h_update(double2* H, const double2* adv, const double2* phi, size_t S, int M, double c1, double dt,
-              double bcoef, double sinsl, double cossl, int sdir, double dtf1, double dtf2, cudaStream_t s);
+              double bcoef, double sinsl, double cossl, int sdir, double dtf1, double dtf2, const double* dtf,
+              cudaStream_t s);
 void axmby(double2* y, const double2* x, size_t n, double a, double b, cudaStream_t s);
 void boundary_apply(double2* rhs, const double2* hist, size_t S, int M, int nz, double fac, double r, int opentop,
                     double tu, double tv, double tw, cudaStream_t s);

@@ -114,6 +114,10 @@ class ChannelCase:
                                     ctypes.byref(done)))
         return done.value
 
+    def set_graphs(self, enable: bool):
+        """Replay whole RK3 steps of run_steps as CUDA graphs (default) or not."""
+        check(self.lib.tg_set_graphs(self.h, int(bool(enable))))
+
     def features(self) -> np.ndarray:
         f = np.zeros(_lib.TG_NFEATURE)
         check(self.lib.tg_features(self.h, _p(f)))
