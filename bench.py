@@ -42,7 +42,90 @@ WORKLOADS = {
     "cfg1": dict(nx=32, ny=32, nz=65, nphase=1, reynolds=180.0, precision="fp64"),
     "cfg5": dict(nx=512, ny=256, nz=257, nphase=2, reynolds=1000.0, precision="mixed", lx=8 * math.pi),
     "small": dict(nx=64, ny=64, nz=65, nphase=2, reynolds=800.0, precision="mixed"),
+    # batched ensemble: 16 cases, grids drawn between 64^2x65 and 192^2x193 (see ensemble_params)
+    "cfg4": dict(nx=64, ny=64, nz=65, nphase=2, reynolds=800.0, precision="mixed"),
 }
+
+
+def ensemble_params(count: int = 16, seed: int = 4) -> list:
+    """Uneven grids and parameters drawn from a seed: Nx = Ny even in [64, 192]
+    with prime factors up to 7 (the FFT-friendly lengths a spectral case uses),
+    Nz = Nx + 1, Re ~ U[400, 1000], Ws ~ logU[1e-4, 1e-3], Schmidt 0.5."""
+    def smooth(n):
+        for q in (2, 3, 5, 7):
+            while n % q == 0:
+                n //= q
+        return n == 1
+    sizes = [n for n in range(64, 193, 2) if smooth(n)]
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        n = int(sizes[rng.integers(0, len(sizes))])
+        p = case_params("cfg4")
+        p.update(nx=n, ny=n, nz=n + 1, reynolds=float(rng.uniform(400.0, 1000.0)),
+                 settling=float(10 ** rng.uniform(-4.0, -3.0)))
+        out.append(p)
+    return out
+
+
+def ensemble_arm(args):
+    """16 independent cases stepped together (tg_run_ensemble, one stream and
+    one step graph per case) against the same cases stepped one after another."""
+    import torch
+    import turbid_b200 as tb
+    from turbid_b200 import synthetic, _lib
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    plist = ensemble_params()
+    lib = _lib.load()
+    cases, streams = [], []
+    for i, p in enumerate(plist):
+        s = torch.cuda.Stream()
+        c = tb.ChannelCase(**dict(p, precision=args.precision or p["precision"]))
+        c.set_stream(s.cuda_stream)
+        uvw, pr, phi = synthetic.initial_state(seed=100 + i, **p)
+        c.upload_state(uvw, pr, phi)
+        c.run_steps(args.warmup)
+        cases.append(c)
+        streams.append(s)
+    torch.cuda.synchronize()
+    base = torch.cuda.Stream()
+
+    def timed(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(base)
+        for s in streams:
+            s.wait_event(e0)
+        fn()
+        for s in streams:
+            ev = torch.cuda.Event()
+            ev.record(s)
+            base.wait_event(ev)
+        e1.record(base)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    sampler = ClockSampler(0)
+    sampler.start()
+    l0 = lib.tg_launch_count()
+    ms = timed(lambda: tb.run_ensemble(cases, args.steps))
+    launches = lib.tg_launch_count() - l0
+    clocks = sampler.stop()
+    ms_seq = timed(lambda: [c.run_steps(args.steps) for c in cases])
+    steps = args.steps * len(cases)
+    points = sum(p["nx"] * p["ny"] * p["nz"] for p in plist)
+    line = {"metric": "ensemble case-steps/sec (16 cases, 64^2x65 .. 192^2x193, sediment)",
+            "value": steps / (ms * 1e-3), "unit": "case-steps/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 transforms/products + f64 z-solves", "data": "synthetic",
+            "config": {"workload": "cfg4 batched ensemble", "cases": [(p["nx"], p["nz"]) for p in plist],
+                       "grid_points": points, "precision": args.precision or "mixed",
+                       "parallelism": "single GPU, one stream and one step graph per case"},
+            "sequential_case_steps_per_s": steps / (ms_seq * 1e-3),
+            "gpu_launches": launches, "clocks": clocks}
+    print(json.dumps(line), flush=True)
+    for c in cases:
+        c.close()
 
 
 def case_params(name: str) -> dict:
@@ -228,7 +311,9 @@ def our_arm(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    stream = torch.cuda.current_stream()
+    # a dedicated stream: whole steps are then replayed as CUDA graphs (the
+    # legacy default stream cannot be captured); events are recorded on it
+    stream = torch.cuda.Stream()
     case = tb.ChannelCase(**dict(params, precision=prec))
     case.set_stream(stream.cuda_stream)
     case.upload_state(uvw0, p0, phi0)
@@ -402,6 +487,8 @@ def main():
     args = ap.parse_args()
     if args.impl == "reference":
         reference_arm(args)
+    elif args.workload == "cfg4":
+        ensemble_arm(args)
     else:
         our_arm(args)
 

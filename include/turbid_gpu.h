@@ -169,6 +169,13 @@ TG_API tg_status tg_run_steps(tg_ctx* ctx, int nsteps, int maxstep, double maxcf
  * kernel separately.  Results are identical either way.  Default: enabled.
  * (No reference counterpart; execution control.) */
 TG_API tg_status tg_set_graphs(tg_ctx* ctx, int enable);
+/* tg_run_steps for n independent cases (each context on its own stream, e.g.
+ * an ensemble of uneven grids and parameters): every case's step is enqueued
+ * before any case's previous features are awaited, so the cases run
+ * concurrently on the GPU.  done[i] (may be NULL) receives the steps case i
+ * took.  (No reference counterpart: the reference runs one case per job.) */
+TG_API tg_status tg_run_ensemble(tg_ctx** ctxs, int n, int nsteps, int maxstep, double maxcfl,
+                                 int* done);
 
 /* Phase::GetFeatureGlobal (src/phase.h:57): 50 doubles, device -> host. */
 TG_API tg_status tg_features(tg_ctx* ctx, double* out);

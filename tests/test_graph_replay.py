@@ -65,3 +65,44 @@ def test_graph_replay_matches_oracle(cuda):
         sol.run_step()
     # the library's own decompositions: 1e-9 (the oracle's numpy eigenvectors differ in round-off)
     assert O.rel_l2(u, sol.uvw) < 1e-9 and O.rel_l2(p, sol.p) < 1e-9 and O.rel_l2(c, sol.phi) < 1e-9
+
+
+def ensemble_cfgs(count, seed, lo=24, hi=48):
+    """Uneven grids and parameters drawn from a seed, as in the batched-ensemble
+    configuration (Nx = Ny even, Nz = Nx + 1, Re ~ U[400, 1000], Ws ~ logU[1e-4, 1e-3])."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        n = int(rng.integers(lo // 2, hi // 2 + 1)) * 2
+        out.append(sediment_cfg(nx=n, ny=n, nz=n + 1, reynolds=float(rng.uniform(400, 1000)),
+                                settling=float(10 ** rng.uniform(-4, -3))))
+    return out
+
+
+def test_ensemble_matches_single_cases(cuda):
+    """tg_run_ensemble (cases on their own streams, stepped together) gives each
+    case exactly the fields of its own tg_run_steps run."""
+    import torch
+    cfgs = ensemble_cfgs(4, seed=5)
+    precisions = ["mixed", "fp64", "mixed", "mixed"]
+    states = [O.make_initial_state(c, seed=40 + i, noise=0.05) for i, c in enumerate(cfgs)]
+    streams = [torch.cuda.Stream() for _ in cfgs]
+
+    def make(i):
+        c = cfgs[i]
+        gc = tb.ChannelCase(precision=precisions[i], **{k: getattr(c, k) for k in CASE_KEYS})
+        gc.set_stream(streams[i].cuda_stream)
+        uvw, p, phi = states[i]
+        gc.upload_state(uvw, p, phi)
+        return gc
+
+    ens = [make(i) for i in range(len(cfgs))]
+    assert tb.run_ensemble(ens, 6) == [6] * len(cfgs)
+    for i in range(len(cfgs)):
+        one = make(i)
+        assert one.run_steps(6) == 6
+        a, b = ens[i].download_state(), one.download_state()
+        for x, y in zip(a, b):
+            assert np.array_equal(x, y), i
+        one.close()
+        ens[i].close()

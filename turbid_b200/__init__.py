@@ -7,4 +7,4 @@ host-side interface for Python callers.
 """
 from ._lib import TgCase, TgError, load, TG_PREC_FP64, TG_PREC_MIXED  # noqa: F401
 from .config import Ini, make_case, params_from_ini, expression  # noqa: F401
-from .solver import ChannelCase, decomposition_host, operators_host, to_slab, from_slab  # noqa: F401
+from .solver import ChannelCase, decomposition_host, operators_host, run_ensemble, to_slab, from_slab  # noqa: F401

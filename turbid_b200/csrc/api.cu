@@ -809,46 +809,92 @@ static void run_step_graph(Ctx& x) {
   g_launches += x.gkernels[par];
 }
 
-static int run_steps(Ctx& x, int nsteps, int maxstep, double maxcfl, double* feat_out) {
-  if (!x.loaded) throw Error{TG_ERR_STATE, "FlatChannelSolver::Execute > state not loaded"};
-  int done = 0;
-  int pending = -1;           // slot of the feature copy of the previous step
-  double prev_f19 = x.feat_h[50 + 19];
-  for (int k = 0; k < nsteps && x.isforward; ++k) {
-    // TimeStepper::Update (src/stepper_time.cc:72-113); the CFL uses the features of
-    // the previous step, which are only needed once this step is enqueued.
-    x.step += 1;
-    x.time = x.time + x.dt;
-    bool fwd_flag = x.step < maxstep;
-    if (graph_eligible(x))
-      run_step_graph(x);
-    else if (x.mixed)
-      for (int st = 0; st < 3; ++st) run_stage<float>(x, st);
-    else
-      for (int st = 0; st < 3; ++st) run_stage<double>(x, st);
-    x.alternation = !x.alternation;
-    const int slot = done & 1;
-    TG_CUDA(cudaMemcpyAsync(x.feat_h + slot * 100, x.feat, 100 * sizeof(double), cudaMemcpyDeviceToHost, x.s));
-    TG_CUDA(cudaEventRecord(x.fev[slot], x.s));
-    if (pending >= 0) {
-      TG_CUDA(cudaEventSynchronize(x.fev[pending]));
-      prev_f19 = x.feat_h[pending * 100 + 50 + 19];
-    }
-    x.cfl = prev_f19 * x.dt;
-    if (!std::isfinite(prev_f19)) throw Error{TG_ERR_NAN, "TimeStepper::Update > non-finite CFL feature"};
-    if (x.cfl > maxcfl) fwd_flag = false;
-    x.isforward = fwd_flag;
-    pending = slot;
-    ++done;
+// One step of the Execute loop body, enqueued: TimeStepper::Update's time
+// advance, three stages of both phases, alternation flip, and the feature
+// copy into pinned slot `slot`.
+static void enqueue_step(Ctx& x, int slot) {
+  x.step += 1;
+  x.time = x.time + x.dt;
+  if (graph_eligible(x))
+    run_step_graph(x);
+  else if (x.mixed)
+    for (int st = 0; st < 3; ++st) run_stage<float>(x, st);
+  else
+    for (int st = 0; st < 3; ++st) run_stage<double>(x, st);
+  x.alternation = !x.alternation;
+  TG_CUDA(cudaMemcpyAsync(x.feat_h + slot * 100, x.feat, 100 * sizeof(double), cudaMemcpyDeviceToHost, x.s));
+  TG_CUDA(cudaEventRecord(x.fev[slot], x.s));
+}
+
+// Per-case state of the pipelined step loop: the CFL guard of step k uses the
+// features of step k-1, which are read only after step k has been enqueued.
+struct StepLoop {
+  int done = 0, pending = -1;
+  double prev_f19 = 0.0;
+};
+
+static void check_step(Ctx& x, StepLoop& L, int maxstep, double maxcfl) {
+  bool fwd_flag = x.step < maxstep;
+  if (L.pending >= 0) {
+    TG_CUDA(cudaEventSynchronize(x.fev[L.pending]));
+    L.prev_f19 = x.feat_h[L.pending * 100 + 50 + 19];
   }
+  x.cfl = L.prev_f19 * x.dt;
+  if (!std::isfinite(L.prev_f19)) throw Error{TG_ERR_NAN, "TimeStepper::Update > non-finite CFL feature"};
+  if (x.cfl > maxcfl) fwd_flag = false;
+  x.isforward = fwd_flag;
+  L.pending = L.done & 1;
+  ++L.done;
+}
+
+static void finish_steps(Ctx& x, StepLoop& L, double* feat_out) {
   TG_CUDA(cudaStreamSynchronize(x.s));
-  if (pending >= 0) {
-    std::memcpy(x.feat_h + 100 * (pending ^ 1), x.feat_h + 100 * pending, 100 * sizeof(double));
-    if (feat_out) std::memcpy(feat_out, x.feat_h + pending * 100 + 50, 50 * sizeof(double));
-    if (!std::isfinite(x.feat_h[pending * 100 + 50 + 19]))
+  if (L.pending >= 0) {
+    std::memcpy(x.feat_h + 100 * (L.pending ^ 1), x.feat_h + 100 * L.pending, 100 * sizeof(double));
+    if (feat_out) std::memcpy(feat_out, x.feat_h + L.pending * 100 + 50, 50 * sizeof(double));
+    if (!std::isfinite(x.feat_h[L.pending * 100 + 50 + 19]))
       throw Error{TG_ERR_NAN, "FlatCarrierPhase::Correct > non-finite velocity features"};
   }
-  return done;
+}
+
+static int run_steps(Ctx& x, int nsteps, int maxstep, double maxcfl, double* feat_out) {
+  if (!x.loaded) throw Error{TG_ERR_STATE, "FlatChannelSolver::Execute > state not loaded"};
+  StepLoop L;
+  L.prev_f19 = x.feat_h[50 + 19];
+  for (int k = 0; k < nsteps && x.isforward; ++k) {
+    enqueue_step(x, L.done & 1);
+    check_step(x, L, maxstep, maxcfl);
+  }
+  finish_steps(x, L, feat_out);
+  return L.done;
+}
+
+// Independent cases stepped together: each step of every case is enqueued on
+// its own stream before the previous step's features of any case are awaited,
+// so the cases' kernels (or step graphs) overlap on the GPU.
+static void run_ensemble(std::vector<Ctx*>& xs, int nsteps, int maxstep, double maxcfl, int* done) {
+  std::vector<StepLoop> L(xs.size());
+  for (size_t i = 0; i < xs.size(); ++i) {
+    if (!xs[i]->loaded) throw Error{TG_ERR_STATE, "FlatChannelSolver::Execute > state not loaded"};
+    L[i].prev_f19 = xs[i]->feat_h[50 + 19];
+  }
+  for (int k = 0; k < nsteps; ++k) {
+    bool any = false;
+    std::vector<char> stepped(xs.size(), 0);
+    for (size_t i = 0; i < xs.size(); ++i)
+      if (xs[i]->isforward) {
+        enqueue_step(*xs[i], L[i].done & 1);
+        stepped[i] = 1;
+        any = true;
+      }
+    if (!any) break;
+    for (size_t i = 0; i < xs.size(); ++i)
+      if (stepped[i]) check_step(*xs[i], L[i], maxstep, maxcfl);
+  }
+  for (size_t i = 0; i < xs.size(); ++i) {
+    finish_steps(*xs[i], L[i], nullptr);
+    if (done) done[i] = L[i].done;
+  }
 }
 
 }  // namespace tg
@@ -1109,6 +1155,22 @@ tg_status tg_set_graphs(tg_ctx* ctx, int enable) {
   x.graphs = enable != 0;
   if (!x.graphs) x.drop_graphs();
   return TG_OK;
+}
+
+tg_status tg_run_ensemble(tg_ctx** ctxs, int n, int nsteps, int maxstep, double maxcfl, int* done) {
+  if (!ctxs || n < 1) {
+    set_error("tg_run_ensemble > bad argument");
+    return TG_ERR_ARG;
+  }
+  std::vector<Ctx*> xs(n);
+  for (int i = 0; i < n; ++i) {
+    if (!ctxs[i]) {
+      set_error("tg_run_ensemble > null context");
+      return TG_ERR_ARG;
+    }
+    xs[i] = reinterpret_cast<Ctx*>(ctxs[i]);
+  }
+  TG_TRY(run_ensemble(xs, nsteps, maxstep, maxcfl, done));
 }
 
 tg_status tg_run_steps(tg_ctx* ctx, int nsteps, int maxstep, double maxcfl, double* features, int* done) {

@@ -186,3 +186,14 @@ def to_slab(ref: np.ndarray) -> np.ndarray:
 def from_slab(slab: np.ndarray, nxh: int, nyc: int) -> np.ndarray:
     d, nz, M = slab.shape
     return np.ascontiguousarray(slab.transpose(0, 2, 1).reshape(d, nxh, nyc, nz))
+
+
+def run_ensemble(cases, nsteps: int, maxstep: int = 2 ** 30, maxcfl: float = 1e300):
+    """tg_run_ensemble: nsteps RK3 steps of independent cases stepped together
+    (each on its own stream); returns the steps each case took."""
+    lib = _lib.load()
+    n = len(cases)
+    handles = (ctypes.c_void_p * n)(*[c.h.value if isinstance(c.h, ctypes.c_void_p) else c.h for c in cases])
+    done = (ctypes.c_int * n)()
+    check(lib.tg_run_ensemble(handles, n, int(nsteps), int(maxstep), float(maxcfl), done))
+    return list(done)
