@@ -231,43 +231,83 @@ void boundary_apply(double2* rhs, const double2* hist, size_t S, int M, int nz, 
 // FlatCarrierBoundary::Update (boundary_carrier_flat.cc:131-170): history
 // shift and new wall rows of grad p; with an open top the rows of grad(dp/dz)
 // (phase_carrier_flat.cc:599-604) where only rows 0 and N-1 are needed.
+// Rows 0 and N-1 of D1*f for columns [m0, m0+32) of one component: the z sum
+// is split over the 8 thread rows of a (32 x 8) block (each a strided subset
+// of z, loads coalesced along m) and reduced in shared memory.  Thread row 0
+// returns the two sums of its column.
+__device__ __forceinline__ void wall_rows_d1(const double2* __restrict__ f, int M, int nz, int m,
+                                            const double* __restrict__ d1r0, const double* __restrict__ d1rn,
+                                            double2& r0, double2& rn) {
+  __shared__ double part[8][32][4];
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  double a = 0, b = 0, c = 0, d = 0;
+  if (m < M) {
+#pragma unroll 4
+    for (int k = ty; k < nz; k += 8) {
+      const double2 v = f[(size_t)k * M + m];
+      a += d1r0[k] * v.x;
+      b += d1r0[k] * v.y;
+      c += d1rn[k] * v.x;
+      d += d1rn[k] * v.y;
+    }
+  }
+  part[ty][tx][0] = a;
+  part[ty][tx][1] = b;
+  part[ty][tx][2] = c;
+  part[ty][tx][3] = d;
+  __syncthreads();
+  if (ty == 0) {
+    for (int j = 1; j < 8; ++j) {
+      a += part[j][tx][0];
+      b += part[j][tx][1];
+      c += part[j][tx][2];
+      d += part[j][tx][3];
+    }
+    r0 = make_double2(a, b);
+    rn = make_double2(c, d);
+  }
+  __syncthreads();
+}
+
+// FlatCarrierBoundary::Update (boundary_carrier_flat.cc:131-170): shift the
+// history rows, store the new pressure-gradient wall rows; with an open top
+// also d(dp/dz)/dz at the walls (rows 0, N-1 of D1 applied to dp/dz).
+// Block (32, 8): 32 columns, 8 rows of the z sum.
 __global__ void k_boundary_update(double2* __restrict__ hist, const double2* __restrict__ dp, size_t S, int M, int nz,
                                   int opentop, const double* __restrict__ kx, const double* __restrict__ ky,
                                   const double* __restrict__ d1r0, const double* __restrict__ d1rn) {
   const size_t R = (size_t)3 * M;
-  for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < M; m += gridDim.x * blockDim.x) {
-    for (int c = 0; c < 3; ++c) {
-      const size_t i = (size_t)c * M + m;
-      hist[2 * R + i] = hist[0 * R + i];
-      hist[3 * R + i] = hist[1 * R + i];
-      hist[6 * R + i] = hist[4 * R + i];
-      hist[7 * R + i] = hist[5 * R + i];
-      hist[1 * R + i] = dp[(size_t)c * S + m];
-      hist[0 * R + i] = dp[(size_t)c * S + (size_t)(nz - 1) * M + m];
-    }
-    if (opentop) {
-      const double2* g = dp + 2 * S;  // dp/dz
-      double2 g0 = g[m], gn = g[(size_t)(nz - 1) * M + m];
-      double s0x = 0, s0y = 0, snx = 0, sny = 0;
-      for (int k = 0; k < nz; ++k) {
-        double2 v = g[(size_t)k * M + m];
-        s0x += d1r0[k] * v.x;
-        s0y += d1r0[k] * v.y;
-        snx += d1rn[k] * v.x;
-        sny += d1rn[k] * v.y;
-      }
+  const int m = blockIdx.x * 32 + threadIdx.x;
+  if (threadIdx.y < 3 && m < M) {
+    const int c = threadIdx.y;
+    const size_t i = (size_t)c * M + m;
+    hist[2 * R + i] = hist[0 * R + i];
+    hist[3 * R + i] = hist[1 * R + i];
+    hist[6 * R + i] = hist[4 * R + i];
+    hist[7 * R + i] = hist[5 * R + i];
+    hist[1 * R + i] = dp[(size_t)c * S + m];
+    hist[0 * R + i] = dp[(size_t)c * S + (size_t)(nz - 1) * M + m];
+  }
+  if (opentop) {
+    const double2* g = dp + 2 * S;  // dp/dz
+    double2 r0, rn;
+    wall_rows_d1(g, M, nz, m, d1r0, d1rn, r0, rn);
+    if (threadIdx.y == 0 && m < M) {
+      const double2 g0 = g[m], gn = g[(size_t)(nz - 1) * M + m];
       hist[5 * R + 0 * M + m] = mul_i(kx[m], g0);
       hist[5 * R + 1 * M + m] = mul_i(ky[m], g0);
-      hist[5 * R + 2 * M + m] = make_double2(s0x, s0y);
+      hist[5 * R + 2 * M + m] = r0;
       hist[4 * R + 0 * M + m] = mul_i(kx[m], gn);
       hist[4 * R + 1 * M + m] = mul_i(ky[m], gn);
-      hist[4 * R + 2 * M + m] = make_double2(snx, sny);
+      hist[4 * R + 2 * M + m] = rn;
     }
   }
 }
 void boundary_update(double2* hist, const double2* dp, size_t S, int M, int nz, int opentop, const double* kx,
                      const double* ky, const double* d1r0, const double* d1rn, cudaStream_t s) {
-  k_boundary_update<<<nblk(M), kT, 0, s>>>(hist, dp, S, M, nz, opentop, kx, ky, d1r0, d1rn);
+  prof_begin(s, PC_ELEM, 16.0 * (double)M * (opentop ? nz + 16 : 16), 0);
+  k_boundary_update<<<(M + 31) / 32, dim3(32, 8), 0, s>>>(hist, dp, S, M, nz, opentop, kx, ky, d1r0, d1rn);
+  prof_end(s);
   TG_LAUNCH_CHECK("k_boundary_update");
 }
 
@@ -277,26 +317,20 @@ void boundary_update(double2* hist, const double2* dp, size_t S, int M, int nz, 
 // features, phase_carrier_flat.cc:687-692).
 __global__ void k_wall_dz(const double2* __restrict__ U, double2* __restrict__ DU, size_t S, int M, int nz,
                           const double* __restrict__ d1r0, const double* __restrict__ d1rn) {
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < 3 * M; t += gridDim.x * blockDim.x) {
-    const int c = t / M, m = t - c * M;
-    const double2* u = U + (size_t)c * S + m;
-    double s0x = 0, s0y = 0, snx = 0, sny = 0;
-    for (int k = 0; k < nz; ++k) {
-      double2 v = u[(size_t)k * M];
-      s0x += d1r0[k] * v.x;
-      s0y += d1r0[k] * v.y;
-      snx += d1rn[k] * v.x;
-      sny += d1rn[k] * v.y;
-    }
+  const int c = blockIdx.y;
+  const int m = blockIdx.x * 32 + threadIdx.x;
+  double2 r0, rn;
+  wall_rows_d1(U + (size_t)c * S, M, nz, m, d1r0, d1rn, r0, rn);
+  if (threadIdx.y == 0 && m < M) {
     double2* dz = DU + (size_t)(3 * c + 2) * S + m;
-    dz[0] = make_double2(s0x, s0y);
-    dz[(size_t)(nz - 1) * M] = make_double2(snx, sny);
+    dz[0] = r0;
+    dz[(size_t)(nz - 1) * M] = rn;
   }
 }
 void wall_dz(const double2* U, double2* DU, size_t S, int M, int nz, const double* d1r0, const double* d1rn,
              cudaStream_t s) {
   prof_begin(s, PC_ELEM, 3.0 * 16.0 * (double)S, 0);
-  k_wall_dz<<<nblk(3 * (size_t)M), kT, 0, s>>>(U, DU, S, M, nz, d1r0, d1rn);
+  k_wall_dz<<<dim3((M + 31) / 32, 3), dim3(32, 8), 0, s>>>(U, DU, S, M, nz, d1r0, d1rn);
   prof_end(s);
   TG_LAUNCH_CHECK("k_wall_dz");
 }
@@ -433,31 +467,31 @@ void positivity_filter(T* phip, int plane_n, int nz, cudaStream_t s) {
 template <typename T>
 __global__ void k_feature_max(const T* __restrict__ unl, int nx, int ny, int nz, const double* __restrict__ glz,
                               double lmx, double lmy, unsigned long long* bits) {
+  // blockIdx.y = z plane: the wall maxima and 1/glz need no per-element index division
   const size_t plane = (size_t)nx * ny, P = plane * nz;
-  double mx[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < P; i += (size_t)gridDim.x * blockDim.x) {
-    const int z = (int)(i / plane);
-    double u = fabs((double)unl[i]), v = fabs((double)unl[P + i]), w = fabs((double)unl[2 * P + i]);
-    mx[0] = fmax(mx[0], u);
-    mx[1] = fmax(mx[1], v);
-    mx[2] = fmax(mx[2], w);
-    if (z == 0) {
-      mx[3] = fmax(mx[3], u);
-      mx[4] = fmax(mx[4], v);
-      mx[5] = fmax(mx[5], w);
-    }
-    if (z == nz - 1) {
-      mx[6] = fmax(mx[6], u);
-      mx[7] = fmax(mx[7], v);
-      mx[8] = fmax(mx[8], w);
-    }
-    mx[9] = fmax(mx[9], u / lmx + v / lmy + w / glz[z]);
+  const int z = blockIdx.y;
+  const double gl = glz[z];
+  const T* pu = unl + (size_t)z * plane;
+  double mu = 0, mv = 0, mw = 0, ml = 0;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < plane; i += (size_t)gridDim.x * blockDim.x) {
+    const double u = fabs((double)pu[i]), v = fabs((double)pu[P + i]), w = fabs((double)pu[2 * P + i]);
+    mu = fmax(mu, u);
+    mv = fmax(mv, v);
+    mw = fmax(mw, w);
+    ml = fmax(ml, u / lmx + v / lmy + w / gl);
   }
+  double mx[4] = {mu, mv, mw, ml};
 #pragma unroll
-  for (int k = 0; k < 10; ++k) {
-    double v = mx[k];
-    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
-    if ((threadIdx.x & 31) == 0) atomicMax(bits + k, (unsigned long long)__double_as_longlong(v));
+  for (int k = 0; k < 4; ++k)
+    for (int o = 16; o > 0; o >>= 1) mx[k] = fmax(mx[k], __shfl_down_sync(0xffffffffu, mx[k], o));
+  if ((threadIdx.x & 31) == 0) {
+    for (int k = 0; k < 3; ++k) {
+      const unsigned long long b = (unsigned long long)__double_as_longlong(mx[k]);
+      atomicMax(bits + k, b);
+      if (z == 0) atomicMax(bits + 3 + k, b);
+      if (z == nz - 1) atomicMax(bits + 6 + k, b);
+    }
+    atomicMax(bits + 9, (unsigned long long)__double_as_longlong(mx[3]));
   }
 }
 // flocal = feat[0..49], fglobal = feat[50..99]
@@ -480,7 +514,9 @@ void features(const T* unl, int nx, int ny, int nz, const double* glz, double lm
   TG_CUDA(cudaMemsetAsync(bits, 0, 10 * sizeof(unsigned long long), s));
   size_t P = (size_t)nx * ny * nz;
   prof_begin(s, PC_FEAT, 3.0 * sizeof(T) * (double)P, 0);
-  k_feature_max<T><<<nblk(P, 4), kT, 0, s>>>(unl, nx, ny, nz, glz, lmx, lmy, bits);
+  const size_t plane = (size_t)nx * ny;
+  const unsigned bx = (unsigned)std::max<size_t>(1, std::min<size_t>((plane + 4 * kT - 1) / (4 * kT), 64));
+  k_feature_max<T><<<dim3(bx, nz), kT, 0, s>>>(unl, nx, ny, nz, glz, lmx, lmy, bits);
   prof_end(s);
   TG_LAUNCH_CHECK("k_feature_max");
   k_feature_final<<<1, 32, 0, s>>>(feat, bits, du, S, M, nz);
@@ -491,15 +527,18 @@ void features(const T* unl, int nx, int ny, int nz, const double* glz, double lm
 // phase_carrier_flat.cc:509, phase_scalar_flat.cc:485-518)
 __global__ void k_trapz_mean(const double2* __restrict__ f, int M, int nz, const double* __restrict__ gz, double shift,
                              double* feat, int slot) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  // one warp: lane-strided intervals, then a shuffle sum
   double s = 0.0;
-  for (int k = 0; k < nz - 1; ++k)
+  for (int k = threadIdx.x; k < nz - 1; k += 32)
     s += (gz[k + 1] - gz[k]) * ((f[(size_t)k * M].x + shift) + (f[(size_t)(k + 1) * M].x + shift));
-  feat[slot] = s / 2 / 2;
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if (threadIdx.x == 0) feat[slot] = s / 2 / 2;
 }
 void trapz_mean(const double2* f, int M, int nz, const double* gz, double shift, double* feat, int slot,
                 cudaStream_t s) {
+  prof_begin(s, PC_FEAT, 16.0 * (double)nz, 0);
   k_trapz_mean<<<1, 32, 0, s>>>(f, M, nz, gz, shift, feat, slot);
+  prof_end(s);
   TG_LAUNCH_CHECK("k_trapz_mean");
 }
 
