@@ -111,6 +111,16 @@ struct Ctx {
   cudaStream_t cap_s = nullptr;
   double* force_d = nullptr;  // device [2]
   double* force_h = nullptr;  // pinned [2 parities][2]
+  // The scalar phase's Correct of stage s runs on a second stream s2 while the
+  // carrier's next Predict computes its nonlinear term on s; the carrier waits
+  // for the scalar (sc_done) only where it needs phi (the buoyancy term of the
+  // H update).  The scalar phase then works in its own scratch fields; the
+  // erosion planes alternate between two buffers by stage parity.
+  bool overlap = true, overlap_active = false, sc_pending = false;
+  cudaStream_t s2 = nullptr;
+  cudaEvent_t cc_done = nullptr, sc_done = nullptr;
+  double2 *TMP_s = nullptr, *F6_s = nullptr;
+  void *PRD_s = nullptr, *DUP_s = nullptr, *work_s = nullptr, *PLN2 = nullptr, *PLN1 = nullptr;
   std::vector<void*> allocs;
   Profiler prof;
   // time / phase state
@@ -130,6 +140,13 @@ struct Ctx {
     TG_CUDA(cudaMemset(p, 0, n * sizeof(X)));
     return reinterpret_cast<X*>(p);
   }
+  void release_overlap() {
+    if (s2) cudaStreamDestroy(s2);
+    if (cc_done) cudaEventDestroy(cc_done);
+    if (sc_done) cudaEventDestroy(sc_done);
+    s2 = nullptr;
+    cc_done = sc_done = nullptr;
+  }
   void drop_graphs() {
     for (auto& g : gexec) {
       if (g) cudaGraphExecDestroy(g);
@@ -138,6 +155,7 @@ struct Ctx {
   }
   ~Ctx() {
     drop_graphs();
+    release_overlap();
     if (cap_s) cudaStreamDestroy(cap_s);
     for (void* p : allocs) cudaFree(p);
     if (feat_h) cudaFreeHost(feat_h);
@@ -327,6 +345,18 @@ static Ctx* create(const tg_case& c) {
   // batch so its intermediate stays in L2 measured slower (partial last waves)
   x.work_planes = 9 * x.nz;
   x.work = x.dalloc<double2>((size_t)x.work_planes * x.nxh * x.ny);
+  x.PLN1 = x.PLN;
+  if (x.scalar) {  // the scalar phase's own scratch for the overlapped Correct
+    x.TMP_s = x.dalloc<double2>(3 * S);
+    x.F6_s = x.dalloc<double2>(3 * S);
+    x.PRD_s = x.dalloc<unsigned char>(3 * P * ps);
+    x.DUP_s = x.dalloc<unsigned char>(3 * P * ps);
+    x.work_s = x.dalloc<double2>((size_t)3 * x.nz * x.nxh * x.ny);
+    x.PLN2 = x.dalloc<unsigned char>(3 * (size_t)x.nx * x.ny * ps);
+    TG_CUDA(cudaStreamCreateWithFlags(&x.s2, cudaStreamNonBlocking));
+    TG_CUDA(cudaEventCreateWithFlags(&x.cc_done, cudaEventDisableTiming));
+    TG_CUDA(cudaEventCreateWithFlags(&x.sc_done, cudaEventDisableTiming));
+  }
   x.feat = x.dalloc<double>(100);
   x.bits = x.dalloc<unsigned long long>(16);
   TG_CUDA(cudaMallocHost(&x.feat_h, 2 * 100 * sizeof(double)));
@@ -471,6 +501,10 @@ static void carrier_predict(Ctx& x, int stage) {
   }
   double f1, f2;
   mean_force(x, f1, f2);
+  if (x.sc_pending) {  // phi of the previous stage's scalar Correct (second stream)
+    TG_CUDA(cudaStreamWaitEvent(x.s, x.sc_done, 0));
+    x.sc_pending = false;
+  }
   h_update(x.H, x.ADV, phi, S, x.M, c1, dt, bcoef, std::sin(x.c.slope), std::cos(x.c.slope), x.c.slope_direction,
            dt * f1, dt * f2, x.capturing ? x.force_d : nullptr, x.s);
   // Laplacian and rhs (phase_carrier_flat.cc:517-536)
@@ -680,12 +714,49 @@ static void scalar_correct(Ctx& x, int stage) {
 
 template <typename T>
 static void run_stage(Ctx& x, int stage) {
+  const bool ov = x.overlap_active && x.scalar;
+  if (ov) x.PLN = (stage & 1) ? x.PLN2 : x.PLN1;  // erosion planes of this stage
   carrier_predict<T>(x, stage);
   carrier_correct<T>(x, stage);
   if (x.scalar) {
     scalar_predict(x, stage);
-    scalar_correct<T>(x, stage);
+    if (!ov) {
+      scalar_correct<T>(x, stage);
+    } else {
+      // fork: the scalar Correct on s2, in its own scratch fields
+      TG_CUDA(cudaEventRecord(x.cc_done, x.s));
+      TG_CUDA(cudaStreamWaitEvent(x.s2, x.cc_done, 0));
+      cudaStream_t s1 = x.s;
+      double2 *tmp = x.TMP, *f6 = x.F6;
+      void *prd = x.PRD, *dup = x.DUP, *work = x.work;
+      const int wp = x.work_planes;
+      x.s = x.s2;
+      x.TMP = x.TMP_s;
+      x.F6 = x.F6_s;
+      x.PRD = x.PRD_s;
+      x.DUP = x.DUP_s;
+      x.work = x.work_s;
+      x.work_planes = 3 * x.nz;
+      try {
+        scalar_correct<T>(x, stage);
+      } catch (...) {
+        x.s = s1, x.TMP = tmp, x.F6 = f6, x.PRD = prd, x.DUP = dup, x.work = work, x.work_planes = wp;
+        throw;
+      }
+      x.s = s1, x.TMP = tmp, x.F6 = f6, x.PRD = prd, x.DUP = dup, x.work = work, x.work_planes = wp;
+      TG_CUDA(cudaEventRecord(x.sc_done, x.s2));
+      x.sc_pending = true;
+    }
   }
+}
+
+// After the last stage of a step: the second stream rejoins the first.
+static void join_scalar(Ctx& x) {
+  if (x.sc_pending) {
+    TG_CUDA(cudaStreamWaitEvent(x.s, x.sc_done, 0));
+    x.sc_pending = false;
+  }
+  x.PLN = x.PLN1;
 }
 
 static void upload_state(Ctx& x, const double* uvw, const double* p, const double* phi, int start_step) {
@@ -754,7 +825,17 @@ static bool graph_eligible(const Ctx& x) {
 
 template <typename T>
 static void record_step(Ctx& x) {
-  for (int st = 0; st < 3; ++st) run_stage<T>(x, st);
+  x.overlap_active = x.overlap && x.scalar && !g_prof;  // profiled steps run sequentially
+  try {
+    for (int st = 0; st < 3; ++st) run_stage<T>(x, st);
+    join_scalar(x);  // a captured step ends joined
+  } catch (...) {
+    x.overlap_active = false;
+    x.sc_pending = false;
+    x.PLN = x.PLN1;
+    throw;
+  }
+  x.overlap_active = false;
 }
 
 static void run_step_graph(Ctx& x) {
@@ -815,12 +896,22 @@ static void run_step_graph(Ctx& x) {
 static void enqueue_step(Ctx& x, int slot) {
   x.step += 1;
   x.time = x.time + x.dt;
-  if (graph_eligible(x))
+  if (graph_eligible(x)) {
     run_step_graph(x);
-  else if (x.mixed)
-    for (int st = 0; st < 3; ++st) run_stage<float>(x, st);
-  else
-    for (int st = 0; st < 3; ++st) run_stage<double>(x, st);
+  } else {
+    x.overlap_active = x.overlap && x.scalar && !g_prof;  // profiled steps run sequentially
+    try {
+      if (x.mixed)
+        for (int st = 0; st < 3; ++st) run_stage<float>(x, st);
+      else
+        for (int st = 0; st < 3; ++st) run_stage<double>(x, st);
+      join_scalar(x);
+    } catch (...) {
+      x.overlap_active = false;
+      throw;
+    }
+    x.overlap_active = false;
+  }
   x.alternation = !x.alternation;
   TG_CUDA(cudaMemcpyAsync(x.feat_h + slot * 100, x.feat, 100 * sizeof(double), cudaMemcpyDeviceToHost, x.s));
   TG_CUDA(cudaEventRecord(x.fev[slot], x.s));

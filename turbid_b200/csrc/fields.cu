@@ -484,7 +484,16 @@ __global__ void k_feature_max(const T* __restrict__ unl, int nx, int ny, int nz,
 #pragma unroll
   for (int k = 0; k < 4; ++k)
     for (int o = 16; o > 0; o >>= 1) mx[k] = fmax(mx[k], __shfl_down_sync(0xffffffffu, mx[k], o));
-  if ((threadIdx.x & 31) == 0) {
+  // block maximum first: one atomic per block and value (the values are
+  // non-negative, so their bit patterns order like the numbers)
+  __shared__ double wm[32][4];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  if (lane == 0)
+    for (int k = 0; k < 4; ++k) wm[warp][k] = mx[k];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < nw; ++w)
+      for (int k = 0; k < 4; ++k) mx[k] = fmax(mx[k], wm[w][k]);
     for (int k = 0; k < 3; ++k) {
       const unsigned long long b = (unsigned long long)__double_as_longlong(mx[k]);
       atomicMax(bits + k, b);
@@ -515,7 +524,7 @@ void features(const T* unl, int nx, int ny, int nz, const double* glz, double lm
   size_t P = (size_t)nx * ny * nz;
   prof_begin(s, PC_FEAT, 3.0 * sizeof(T) * (double)P, 0);
   const size_t plane = (size_t)nx * ny;
-  const unsigned bx = (unsigned)std::max<size_t>(1, std::min<size_t>((plane + 4 * kT - 1) / (4 * kT), 64));
+  const unsigned bx = (unsigned)std::max<size_t>(1, std::min<size_t>((plane + 16 * kT - 1) / (16 * kT), 8));
   k_feature_max<T><<<dim3(bx, nz), kT, 0, s>>>(unl, nx, ny, nz, glz, lmx, lmy, bits);
   prof_end(s);
   TG_LAUNCH_CHECK("k_feature_max");
