@@ -177,6 +177,13 @@ TG_API tg_status tg_set_graphs(tg_ctx* ctx, int enable);
 TG_API tg_status tg_run_ensemble(tg_ctx** ctxs, int n, int nsteps, int maxstep, double maxcfl,
                                  int* done);
 
+/* FlatChannelPostprocessor::Execute (src/postprocessor_channel_flat.cc:195-236)
+ * for the current state: swirling strength lambda_ci (largest |Im| of the
+ * eigenvalues of the velocity-gradient tensor du_i/dx_j) at every physical
+ * point, FP64, into vortex[nz][ny][nx] (host; the reference's real cube
+ * layout, x fastest).  Allocates its work buffers on the first call. */
+TG_API tg_status tg_swirling_strength(tg_ctx* ctx, double* vortex);
+
 /* Phase::GetFeatureGlobal (src/phase.h:57): 50 doubles, device -> host. */
 TG_API tg_status tg_features(tg_ctx* ctx, double* out);
 

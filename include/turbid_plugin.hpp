@@ -9,6 +9,8 @@
  *   FlatCarrierVariable  src/variable_carrier_flat.cc:143-377 (Save/Load, IO level one)
  *   FlatChannelSolver    src/solver_channel_flat.cc:31-120 (Configure), :199-293
  *                        (Execute), :372-414 (PrintLogBody)
+ *   FlatChannelPostprocessor  src/postprocessor_channel_flat.cc:153-236 (swirling
+ *                        strength of the saved states, phase_00_vortex.dat)
  *
  * One GPU context (tg_ctx) holds the whole case; the phase objects are views
  * on it that call the per-stage entry points, so the Execute loop below is the
@@ -662,6 +664,55 @@ class FlatChannelSolver {
   std::unique_ptr<GpuCase> gpu_;
   std::unique_ptr<FlatCarrierPhase> carrier_;
   std::unique_ptr<FlatScalarPhase> scalar_;
+  std::unique_ptr<FlatVariables> variables_;
+};
+
+// ---------------------------------------------------------------------------
+// FlatChannelPostprocessor: swirling strength of the saved states
+// [PostProcessor] work_index_range = first last; writes
+// <index>/phase_00_vortex.dat (Armadillo binary real cube, Nx x Ny x Nz)
+// ---------------------------------------------------------------------------
+class FlatChannelPostprocessor {
+ public:
+  FlatChannelPostprocessor(int argc, char** argv) {
+    for (int i = 1; i < argc; ++i) {
+      const std::string a = argv[i];
+      if (a.rfind("--", 0) != 0) {
+        config_ = a;
+        break;
+      }
+    }
+    const size_t slash = config_.find_last_of('/');
+    directory_ = slash == std::string::npos ? "./" : config_.substr(0, slash + 1);
+  }
+  void Configure() {
+    ini_.Load(config_);
+    RunControl rc;
+    gpu_.reset(new GpuCase(CaseFromIni(ini_, rc)));
+    variables_.reset(new FlatVariables(*gpu_));
+    range_ = ini_.GetVectorInt("PostProcessor", "work_index_range");
+    if (range_.size() != 2) throw std::runtime_error("FlatChannelPostprocessor::Configure > work_index_range needs 2 values");
+  }
+  void Execute() {
+    const tg_case& c = gpu_->config();
+    std::vector<double> vortex((size_t)c.nx * c.ny * c.nz);
+    for (int index = range_[0]; index <= range_[1]; ++index) {
+      const std::string path = directory_ + std::to_string((long long)index) + "/";
+      variables_->Load(path, 0);
+      Check("FlatChannelPostprocessor::Execute", tg_swirling_strength(gpu_->ctx(), vortex.data()));
+      std::ofstream f(path + "phase_00_vortex.dat", std::ios::binary);
+      if (!f) throw std::runtime_error("FlatChannelPostprocessor::Execute > Can not Open " + path + "phase_00_vortex.dat");
+      f << "ARMA_CUB_BIN_FN008\n" << c.nx << " " << c.ny << " " << c.nz << "\n";
+      f.write(reinterpret_cast<const char*>(vortex.data()), (std::streamsize)(vortex.size() * sizeof(double)));
+      std::cout << std::setw(12) << index << std::endl;
+    }
+  }
+
+ private:
+  std::string config_ = "configuration.ini", directory_ = "./";
+  IniFile ini_;
+  std::vector<int> range_;
+  std::unique_ptr<GpuCase> gpu_;
   std::unique_ptr<FlatVariables> variables_;
 };
 

@@ -996,3 +996,26 @@ class OracleSolver:
 def rel_l2(a: np.ndarray, b: np.ndarray) -> float:
     den = np.linalg.norm(b.ravel())
     return float(np.linalg.norm((a - b).ravel()) / (den if den > 0 else 1.0))
+
+
+# ----------------------------------------------------------------------------
+# Post-processor: swirling strength (src/postprocessor_channel_flat.cc:195-236)
+# ----------------------------------------------------------------------------
+def swirling_strength(cfg: CaseConfig, uvw: np.ndarray) -> np.ndarray:
+    """lambda_ci per physical point: the largest |imaginary part| of the
+    eigenvalues (eig_gen) of the velocity-gradient tensor A(i, j) = du_i/dx_j,
+    the gradients taken as SpaceStepper::Gradient does (i kx, i ky, D1) and
+    transformed back.  uvw: (3, Nxh, Nyc, Nz) spectral; returns (Nz, Ny, Nx)."""
+    g = Grid(cfg)
+    D1, _ = chebyshev_d1_d2(g, cfg.mapping, cfg.mapping_coef)
+    u = np.asarray(uvw, dtype=np.complex128).reshape(3, g.nxh, g.nyc, g.nz)
+    grads = np.empty((3, 3) + u.shape[1:], dtype=np.complex128)
+    for i in range(3):
+        fm = u[i].reshape(g.M, g.nz)
+        grads[i, 0] = (g.dx1[:, None] * fm).reshape(u.shape[1:])
+        grads[i, 1] = (g.dy1[:, None] * fm).reshape(u.shape[1:])
+        grads[i, 2] = zmul(D1, fm).reshape(u.shape[1:])
+    phys = dft_backward(g, grads.reshape((9,) + u.shape[1:]))        # (9, Nz, Ny, Nx)
+    A = np.moveaxis(phys.reshape(3, 3, -1), -1, 0)                   # (points, 3, 3)
+    ev = np.linalg.eigvals(A)
+    return np.abs(ev.imag).max(axis=1).reshape(g.nz, g.ny, g.nx)

@@ -263,3 +263,24 @@ def test_errors_are_reported(cuda):
     gc.close()
     with pytest.raises(tb.TgError):
         tb.ChannelCase(nx=8, ny=8, nz=9, nphase=3)
+
+
+# ----------------------------------------------------------------------------
+# post-processor
+# ----------------------------------------------------------------------------
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_swirling_strength_matches_oracle(cuda, precision):
+    """lambda_ci of the velocity-gradient tensor at every point (FP64 in both
+    precision modes) against the oracle's numpy eigenvalues."""
+    cfg = sediment_cfg(nx=32, ny=24, nz=33)
+    uvw, p, phi = O.make_initial_state(cfg, seed=12, noise=0.3)
+    gc = gpu_case(cfg, precision)
+    gc.upload_state(uvw, p, phi)
+    got = gc.swirling_strength()
+    ref = O.swirling_strength(cfg, uvw)
+    assert got.shape == ref.shape and ref.max() > 0.1
+    assert rel(got, ref) < 1e-10
+    assert np.abs(got - ref).max() < 1e-9 * ref.max()
+    with pytest.raises(tb.TgError):
+        tb.ChannelCase(nx=8, ny=8, nz=9).swirling_strength()   # no state loaded
+    gc.close()

@@ -225,3 +225,29 @@ def test_driver_runs_case_directory(cuda, driver, tmp_path, nphase):
     # the log line carries the reference's columns: step, time, CFL, features 0..8
     assert float(log[-1][1]) == pytest.approx(sol.time, rel=1e-9)
     np.testing.assert_allclose([float(v) for v in log[-1][3:12]], sol.fglobal[0:9], rtol=1e-5, atol=1e-12)
+
+
+@pytest.mark.gpu
+def test_driver_postprocess(cuda, driver, tmp_path):
+    """--postprocess: the states of [PostProcessor] work_index_range get their
+    swirling strength written as <index>/phase_00_vortex.dat."""
+    cfg = sediment_cfg()
+    write_ini(tmp_path / "configuration.ini", cfg, maxstep=1, writeinterval=1)
+    with open(tmp_path / "configuration.ini", "a") as f:
+        f.write("[PostProcessor]\nwork_index_range = 3 4\n")
+    refs = {}
+    for idx in (3, 4):
+        uvw, p, phi = O.make_initial_state(cfg, seed=50 + idx, noise=0.3)
+        O.write_phase_file(str(tmp_path / str(idx) / "phase_00_variable.dat"), [uvw, p])
+        O.write_phase_file(str(tmp_path / str(idx) / "phase_01_variable.dat"), [phi])
+        refs[idx] = O.swirling_strength(cfg, uvw)
+    r = subprocess.run([driver, "--postprocess", str(tmp_path / "configuration.ini")], capture_output=True,
+                       text=True, cwd=str(tmp_path), timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    for idx, ref in refs.items():
+        with open(tmp_path / str(idx) / "phase_00_vortex.dat", "rb") as f:
+            assert f.readline().strip() == b"ARMA_CUB_BIN_FN008"
+            nx, ny, nz = (int(v) for v in f.readline().split())
+            got = np.frombuffer(f.read(), dtype=np.float64).reshape(nz, ny, nx)
+        assert (nx, ny, nz) == (cfg.nx, cfg.ny, cfg.nz)
+        assert O.rel_l2(got, ref) < 1e-10

@@ -116,6 +116,8 @@ struct Ctx {
   // for the scalar (sc_done) only where it needs phi (the buoyancy term of the
   // H update).  The scalar phase then works in its own scratch fields; the
   // erosion planes alternate between two buffers by stage parity.
+  double *post_buf = nullptr, *post_out = nullptr;  // post-processor, allocated on first use
+  int post_planes = 0;
   bool overlap = true, overlap_active = false, sc_pending = false;
   cudaStream_t s2 = nullptr;
   cudaEvent_t cc_done = nullptr, sc_done = nullptr;
@@ -1238,6 +1240,49 @@ tg_status tg_scalar_predict(tg_ctx* ctx, int stage) {
 tg_status tg_scalar_correct(tg_ctx* ctx, int stage) {
   if (ctx && !has_scalar(ctx)) return TG_ERR_STATE;
   TG_STAGE_CALL(scalar_correct<float>(x, stage), scalar_correct<double>(x, stage));
+}
+
+// FlatChannelPostprocessor::Execute (src/postprocessor_channel_flat.cc:195-236)
+// for the current state: the velocity gradients (SpaceStepper::Gradient, the
+// GEMM with the gradient epilogue), their FP64 c2r in chunks of z planes, and
+// lambda_ci per point.
+static void swirling_strength(Ctx& x, double* out_host) {
+  if (!x.loaded) throw Error{TG_ERR_STATE, "FlatChannelPostprocessor::Execute > state not loaded"};
+  const size_t S = x.S, plane = (size_t)x.nx * x.ny;
+  if (!x.post_buf) {
+    x.post_planes = std::min(x.nz, 16);
+    x.post_buf = x.dalloc<double>(9 * (size_t)x.post_planes * plane);
+    x.post_out = x.dalloc<double>(x.P);
+  }
+  EpiParams ep;
+  ep.mode = EPI_GRAD;
+  ep.kx = x.kx;
+  ep.ky = x.ky;
+  ep.X0 = x.U;
+  ep.sX = S;
+  ep.aux0 = x.DU;
+  ep.aux1 = x.DU + S;
+  ep.sAux = 3 * S;
+  gemm(x, x.opD1, x.U, S, x.DU + 2 * S, 3 * S, 3, ep);
+  const size_t fstride = (size_t)x.post_planes * plane;
+  for (int z0 = 0; z0 < x.nz; z0 += x.post_planes) {
+    const int np = std::min(x.post_planes, x.nz - z0);
+    for (int f = 0; f < 9; ++f)
+      dft_backward<double>(x.td, x.px, x.py, x.DU + (size_t)f * S + (size_t)z0 * x.M, x.post_buf + f * fstride, np,
+                           x.work, x.s);
+    swirling(x.post_buf, fstride, (size_t)np * plane, x.post_out + (size_t)z0 * plane, x.s);
+  }
+  TG_CUDA(cudaMemcpyAsync(out_host, x.post_out, x.P * sizeof(double), cudaMemcpyDeviceToHost, x.s));
+  TG_CUDA(cudaStreamSynchronize(x.s));
+}
+
+tg_status tg_swirling_strength(tg_ctx* ctx, double* vortex) {
+  TG_CHECK_CTX(ctx);
+  if (!vortex) {
+    set_error("FlatChannelPostprocessor::Execute > bad argument");
+    return TG_ERR_ARG;
+  }
+  TG_TRY(swirling_strength(*reinterpret_cast<Ctx*>(ctx), vortex));
 }
 
 tg_status tg_set_graphs(tg_ctx* ctx, int enable) {

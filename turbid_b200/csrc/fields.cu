@@ -580,3 +580,43 @@ INST(float)
 #undef INST
 
 }  // namespace tg
+
+namespace tg {
+
+// Swirling strength (FlatChannelPostprocessor::Execute,
+// src/postprocessor_channel_flat.cc:209-230): lambda_ci = the largest
+// |imaginary part| of the eigenvalues of A(i, j) = du_i/dx_j.  The eigenvalues
+// of a real 3 x 3 matrix are the roots of lambda^3 - P lambda^2 + Q lambda - R
+// (P trace, Q sum of the principal 2 x 2 minors, R determinant); with
+// lambda = t + P/3 the depressed cubic t^3 + p t + q has a complex pair exactly
+// when D = (q/2)^2 + (p/3)^3 > 0, and then (Cardano) the pair is
+// -(u + v)/2 +- i sqrt(3)/2 (u - v) with u = cbrt(-q/2 + sqrt(D)), u v = -p/3.
+__global__ void k_swirling(const double* __restrict__ g, size_t fstride, size_t n, double* __restrict__ out) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    double a[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) a[k] = g[k * fstride + i];
+    const double P = a[0] + a[4] + a[8];
+    const double Q = (a[0] * a[4] - a[1] * a[3]) + (a[0] * a[8] - a[2] * a[6]) + (a[4] * a[8] - a[5] * a[7]);
+    const double R = a[0] * (a[4] * a[8] - a[5] * a[7]) - a[1] * (a[3] * a[8] - a[5] * a[6]) +
+                     a[2] * (a[3] * a[7] - a[4] * a[6]);
+    const double p = Q - P * P / 3.0;
+    const double q = -2.0 * P * P * P / 27.0 + P * Q / 3.0 - R;
+    const double D = 0.25 * q * q + p * p * p / 27.0;
+    double lci = 0.0;
+    if (D > 0.0) {
+      const double s = -0.5 * q;
+      const double u = cbrt(s + copysign(sqrt(D), s));  // the root of larger magnitude
+      const double v = u != 0.0 ? -p / (3.0 * u) : 0.0;
+      lci = 0.86602540378443864676 * fabs(u - v);
+    }
+    out[i] = lci;
+  }
+}
+
+void swirling(const double* grad9, size_t fstride, size_t n, double* out, cudaStream_t s) {
+  k_swirling<<<nblk(n), kT, 0, s>>>(grad9, fstride, n, out);
+  TG_LAUNCH_CHECK("k_swirling");
+}
+
+}  // namespace tg

@@ -40,5 +40,8 @@ void features(const T* unl, int nx, int ny, int nz, const double* glz, double lm
 void trapz_mean(const double2* f, int M, int nz, const double* gz, double shift, double* feat, int slot,
                 cudaStream_t s);
 void set_feat(double* feat, int slot, double v, cudaStream_t s);
+// swirling strength of n points; grad9 holds the nine gradient components
+// du_i/dx_j (index 3 i + j), each fstride doubles apart
+void swirling(const double* grad9, size_t fstride, size_t n, double* out, cudaStream_t s);
 
 }  // namespace tg

@@ -5,6 +5,8 @@
 //
 //   channelflat_gpu [configuration.ini [logcomputation]] [--mixed]
 //   channelflat_gpu --parse-only configuration.ini    (case parameters as JSON, no GPU)
+//   channelflat_gpu --postprocess [configuration.ini]  (swirling strength of the states
+//       of [PostProcessor] work_index_range, written as <index>/phase_00_vortex.dat)
 //   channelflat_gpu --time-only configuration.ini L1 L2 ...
 //       (the time stepper alone for the given per-step maximum velocity/length
 //        values: one JSON line per step with step, time, dt, cfl, flags; no GPU)
@@ -69,6 +71,12 @@ int main(int argc, char** argv) {
                   << ", \"forward\": " << (ts.isForward() ? 1 : 0) << ", \"output\": " << (ts.isOutput() ? 1 : 0)
                   << ", \"output_index\": " << ts.GetOutputTimeIndex() << "}" << std::endl;
       }
+      return 0;
+    }
+    if (argc > 1 && std::string(argv[1]) == "--postprocess") {
+      turbid::FlatChannelPostprocessor post(argc, argv);
+      post.Configure();
+      post.Execute();
       return 0;
     }
     turbid::FlatChannelSolver solver(argc, argv);

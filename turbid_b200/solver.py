@@ -114,6 +114,12 @@ class ChannelCase:
                                     ctypes.byref(done)))
         return done.value
 
+    def swirling_strength(self) -> np.ndarray:
+        """FlatChannelPostprocessor: lambda_ci of the current state, (Nz, Ny, Nx) FP64."""
+        out = np.zeros((self.nz, self.ny, self.nx))
+        check(self.lib.tg_swirling_strength(self.h, _p(out)))
+        return out
+
     def set_graphs(self, enable: bool):
         """Replay whole RK3 steps of run_steps as CUDA graphs (default) or not."""
         check(self.lib.tg_set_graphs(self.h, int(bool(enable))))
