@@ -47,6 +47,23 @@ WORKLOADS = {
 }
 
 
+def replica_max(v: float, dist=None, device: str = "cpu") -> float:
+    """The maximum of a per-rank value over all ranks (the slowest replica's
+    time); dist is torch.distributed (NCCL on the GPU box, gloo in tests)."""
+    if dist is None:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_rate(steps_per_rank: int, ms_max: float, world: int) -> float:
+    """Whole-job throughput of N independent replicas: all ranks' steps over
+    the slowest rank's device time."""
+    return steps_per_rank * world / (ms_max * 1e-3)
+
+
 def ensemble_params(count: int = 16, seed: int = 4) -> list:
     """Uneven grids and parameters drawn from a seed: Nx = Ny even in [64, 192]
     with prime factors up to 7 (the FFT-friendly lengths a spectral case uses),
@@ -305,11 +322,7 @@ def our_arm(args):
         torch.cuda.synchronize()
 
     def max_over_ranks(v):
-        if dist is None:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return replica_max(v, dist, "cuda")
 
     # a dedicated stream: whole steps are then replayed as CUDA graphs (the
     # legacy default stream cannot be captured); events are recorded on it
@@ -334,8 +347,7 @@ def our_arm(args):
     launches = lib.tg_launch_count() - l0
     clocks = sampler.stop() if sampler else None
     ms = max_over_ranks(e0.elapsed_time(e1))
-    total_steps = done * world
-    value = total_steps / (ms * 1e-3)
+    value = replica_rate(done, ms, world)
 
     # ---- kernel classes of the same workload (separate pass, CUDA events per launch)
     case.profile_begin()
