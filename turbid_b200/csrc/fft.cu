@@ -436,6 +436,7 @@ __global__ void __launch_bounds__(NB * L / 16) by_p2_kernel(TransformDims d, con
     buf[c * RS + sp(y)] = mkc<C>(0, 0);
   }
   const double2* src = spec + (size_t)plane * d.M;
+#pragma unroll 4
   for (int idx = threadIdx.x; idx < NB * nyc; idx += NT) {
     const int c = idx / nyc, iy = idx - c * nyc;
     const int k = k0 + c;

@@ -59,6 +59,22 @@ template <typename C> __host__ __device__ __forceinline__ C mkc(decltype(C::x) a
 }
 template <typename C> __device__ __forceinline__ C cadd(C a, C b) { return mkc<C>(a.x + b.x, a.y + b.y); }
 template <typename C> __device__ __forceinline__ C csub(C a, C b) { return mkc<C>(a.x - b.x, a.y - b.y); }
+// complex<float> sums as one packed FP32x2 instruction (sm_100); IEEE
+// round-to-nearest per lane, so the results equal the two scalar operations
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000
+template <> __device__ __forceinline__ float2 cadd<float2>(float2 a, float2 b) {
+  unsigned long long r;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(*reinterpret_cast<unsigned long long*>(&a)),
+      "l"(*reinterpret_cast<unsigned long long*>(&b)));
+  return *reinterpret_cast<float2*>(&r);
+}
+template <> __device__ __forceinline__ float2 csub<float2>(float2 a, float2 b) {
+  unsigned long long r;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(*reinterpret_cast<unsigned long long*>(&a)),
+      "l"(*reinterpret_cast<unsigned long long*>(&b)));
+  return *reinterpret_cast<float2*>(&r);
+}
+#endif
 template <typename C> __device__ __forceinline__ C cmul(C a, C b) {
   return mkc<C>(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
