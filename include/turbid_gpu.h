@@ -216,9 +216,12 @@ TG_API tg_status tg_dft_forward_f32(tg_ctx* ctx, const float* phys, double* spec
  * until exit), so nx and ny must be powers of two in [8, 1024]; larger grids
  * are rejected with TG_ERR_SHAPE.  The first call on each device sets up the
  * static twiddle and index tables on that device (make it with the device
- * current).  All calls share the one scratch array: calls whose work overlaps
- * on the GPU (other streams or other host threads) race; order them on one
- * stream.  Results equal tg_dft_forward_f64's. */
+ * current); that set-up copies the tables with cudaMemcpyToSymbol, so make the
+ * first call on each device before any stream capture begins.  Nothing has to
+ * start at zero: each call writes every scratch element before reading it.
+ * All calls share the one scratch array: calls whose work overlaps on the GPU
+ * (other streams or other host threads) race; order them on one stream.
+ * Results equal tg_dft_forward_f64's. */
 TG_API tg_status tg_dft_forward_f64_noalloc(int nx, int ny, int nz, const double* phys,
                                             double* spec, int dim, void* stream);
 /* RealCplxCube::DftBackward (src/cube_real_cplx.cc:542-555): zero-fill, unscaled. */

@@ -736,6 +736,8 @@ inline int noalloc_offset(int L) { return L - kNoAllocMinL; }
 bool is_supported_pow2(int L) { return L >= kNoAllocMinL && L <= kNoAllocMaxL && (L & (L - 1)) == 0; }
 
 // Per-device set-up, run by the first call on each device (device current).
+// The table copies are synchronous host->device copies, which a stream capture
+// does not allow: the first call on a device must come before any capture.
 NoAllocDevice& noalloc_setup() {
   int dev = 0;
   TG_CUDA(cudaGetDevice(&dev));
