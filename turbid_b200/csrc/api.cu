@@ -178,11 +178,21 @@ static std::function<double*(size_t)> allocator(Ctx& x) {
   return [&x](size_t n) { return x.dalloc<double>(n); };
 }
 
+// The solve's two GEMMs: dense (E^-1 with the forward fix folded in, E with
+// the backward fix rows), or, for a decomposition whose eigenvectors have
+// parity (w and the pressure: the same condition on both walls), the split
+// pair of half-size products of the folded-operator kernel (half the flops).
 static void install_decomposition(Ctx& x, int which) {
   std::vector<double> Ei, E;
-  fold_decomposition(x.dec[which], which == 3, Ei, E);
-  zop_build(x.opEinv[which], Ei, x.nz, false, allocator(x));
-  zop_build(x.opE[which], E, x.nz, false, allocator(x));
+  double quirk = 0.0;
+  if (split_operators(x.dec[which], which == 3, Ei, E, quirk)) {
+    zop_build_split(x.opEinv[which], Ei, x.nz, 1, 0.0, allocator(x));
+    zop_build_split(x.opE[which], E, x.nz, 2, quirk, allocator(x));
+  } else {
+    fold_decomposition(x.dec[which], which == 3, Ei, E);
+    zop_build(x.opEinv[which], Ei, x.nz, false, allocator(x));
+    zop_build(x.opE[which], E, x.nz, false, allocator(x));
+  }
   if (!x.lamd[which]) x.lamd[which] = x.dalloc<double>(x.nz);
   TG_CUDA(cudaMemcpy(x.lamd[which], x.dec[which].lam.data(), sizeof(double) * x.nz, cudaMemcpyHostToDevice));
 }
@@ -1078,6 +1088,7 @@ tg_status tg_set_decomposition(tg_ctx* ctx, int which, const double* E, const do
     d.ftb.assign(ftb, ftb + x.nz);
     d.fbf.assign(fbf, fbf + x.nz);
     d.ftf.assign(ftf, ftf + x.nz);
+    d.parity = false;   // caller's eigenvectors: no parity order assumed, dense solve
     TG_CUDA(cudaStreamSynchronize(x.s));
     install_decomposition(x, which);
   });

@@ -8,6 +8,10 @@
 //           only kx < Nxh kept, written column-major [plane][kx][y];
 //   y pass: complex FFT along y of each kept column, only the Nyc pruned
 //           wavenumbers kept (kx-major), scaled by 1/(Nx*Ny).
+// The backward transform runs the passes in reverse order; in FP32 its
+// intermediate is row-major [plane][y][kx], so that each pass reads contiguous
+// blocks (the strided side of the reorder is a write, which the L2 merges
+// into full lines before they reach HBM).
 // The 1-D FFTs are mixed-radix Stockham passes in shared memory with
 // twiddles from a table computed once per length on the host.
 #include <algorithm>
@@ -136,6 +140,10 @@ __device__ cplx<T>* fft_batch(cplx<T>* b0, cplx<T>* b1, int NB, const PlanArgs& 
   }
   return in;
 }
+
+// Layout of the backward intermediate: [plane][y][kx] for FP32 (the x pass
+// reads contiguous row blocks), [plane][kx][y] for FP64.
+template <typename T> __host__ __device__ constexpr bool bwd_row_major() { return sizeof(T) == 4; }
 
 // ---------------------------------------------------------------------------
 // compile-time Stockham passes for power-of-two lengths: radix-16 passes
@@ -283,13 +291,19 @@ __global__ void __launch_bounds__(256) bwd_y_kernel(TransformDims d, PlanArgs pl
   C* r = fft_any<T, +1, LC>(b0, b1, NB, pl, tw);
   C* dst = work + (size_t)plane * d.nxh * d.ny;
   for (int idx = threadIdx.x; idx < NB * L; idx += blockDim.x) {
-    const int c = idx / L, y = idx - c * L;
-    const int k = k0 + c;
-    if (k < d.nxh) dst[(size_t)k * d.ny + y] = r[idx];
+    if constexpr (bwd_row_major<T>()) {  // [y][kx]
+      const int y = idx / NB, c = idx - y * NB;
+      const int k = k0 + c;
+      if (k < d.nxh) dst[(size_t)y * d.nxh + k] = r[c * L + y];
+    } else {  // [kx][y]
+      const int c = idx / L, y = idx - c * L;
+      const int k = k0 + c;
+      if (k < d.nxh) dst[(size_t)k * d.ny + y] = r[idx];
+    }
   }
 }
 
-// backward x pass: work [plane][kx][y] -> phys [plane][y][x]; two rows per
+// backward x pass: work -> phys [plane][y][x]; two rows per
 // complex FFT; the imaginary part of the kx = 0 coefficient is ignored (c2r).
 template <typename T, int LC>
 __global__ void __launch_bounds__(256) bwd_x_kernel(TransformDims d, PlanArgs pl, const cplx<T>* __restrict__ tw,
@@ -305,10 +319,13 @@ __global__ void __launch_bounds__(256) bwd_x_kernel(TransformDims d, PlanArgs pl
   __syncthreads();
   const C* src = work + (size_t)plane * d.nxh * d.ny;
   for (int idx = threadIdx.x; idx < NB * d.nxh; idx += blockDim.x) {
-    const int k = idx / NB, p = idx - k * NB;
+    constexpr bool RM = bwd_row_major<T>();
+    const int p = RM ? idx / d.nxh : idx % NB, k = RM ? idx - p * d.nxh : idx / NB;
     const int ya = y0 + 2 * p, yb = ya + 1;
-    C h1 = ya < d.ny ? src[(size_t)k * d.ny + ya] : mkc<C>(0, 0);
-    C h2 = yb < d.ny ? src[(size_t)k * d.ny + yb] : mkc<C>(0, 0);
+    const size_t oa = RM ? (size_t)ya * d.nxh + k : (size_t)k * d.ny + ya;
+    const size_t ob = RM ? (size_t)yb * d.nxh + k : (size_t)k * d.ny + yb;
+    C h1 = ya < d.ny ? src[oa] : mkc<C>(0, 0);
+    C h2 = yb < d.ny ? src[ob] : mkc<C>(0, 0);
     if (k == 0) {
       h1.y = T(0);
       h2.y = T(0);
@@ -329,32 +346,69 @@ __global__ void __launch_bounds__(256) bwd_x_kernel(TransformDims d, PlanArgs pl
   }
 }
 
+// Per-precision access widths of the p2 kernels.  FP32: 16-byte vectors (four
+// reals of a row, two complex values of a column) and the backward
+// intermediate row-major [plane][y][kx], so that the backward x pass reads
+// contiguous row blocks.  FP64: one real / one complex value per access and
+// the backward intermediate [plane][kx][y] (measured faster for 16-byte
+// complex values, whose accesses are already wide).
+template <typename T> struct P2Vec;
+template <> struct P2Vec<float> {
+  using R = float4;   // VW reals of a row
+  using CV = float4;  // VC complex values of a column
+  static constexpr int VW = 4, VC = 2;
+  static constexpr bool kBwdRowMajor = bwd_row_major<float>();
+};
+template <> struct P2Vec<double> {
+  using R = double;
+  using CV = double2;
+  static constexpr int VW = 1, VC = 1;
+  static constexpr bool kBwdRowMajor = bwd_row_major<double>();
+};
+__device__ __forceinline__ float vget(const float4& v, int j) { return j == 0 ? v.x : j == 1 ? v.y : j == 2 ? v.z : v.w; }
+__device__ __forceinline__ double vget(const double& v, int) { return v; }
+__device__ __forceinline__ void vset(float4& v, int j, float a) {
+  if (j == 0) v.x = a; else if (j == 1) v.y = a; else if (j == 2) v.z = a; else v.w = a;
+}
+__device__ __forceinline__ void vset(double& v, int, double a) { v = a; }
+__device__ __forceinline__ float2 cget(const float4& v, int j) { return j == 0 ? make_float2(v.x, v.y) : make_float2(v.z, v.w); }
+__device__ __forceinline__ double2 cget(const double2& v, int) { return v; }
+__device__ __forceinline__ void cset(float4& v, int j, float2 a) {
+  if (j == 0) { v.x = a.x; v.y = a.y; } else { v.z = a.x; v.w = a.y; }
+}
+__device__ __forceinline__ void cset(double2& v, int, double2 a) { v = a; }
+template <typename V> __device__ __forceinline__ V vzero() { V v; memset(&v, 0, sizeof(V)); return v; }
+
 // forward x pass, L = nx: NB row pairs per CTA, 2 rows packed per complex FFT
 template <typename T, int L, int NB>
 __global__ void __launch_bounds__(NB * L / 16) fx_p2_kernel(TransformDims d, const cplx<T>* __restrict__ tw,
                                                            const T* __restrict__ phys, cplx<T>* __restrict__ work) {
   using C = cplx<T>;
-  constexpr int RS = P2<L>::RS, NT = NB * L / 16, rows = 2 * NB;
+  using PV = P2Vec<T>;
+  using R = typename PV::R;
+  constexpr int VW = PV::VW, RS = P2<L>::RS, NT = NB * L / 16, rows = 2 * NB;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* buf = reinterpret_cast<C*>(smem_raw);
   const int plane = blockIdx.y;
   const int y0 = blockIdx.x * rows;
   const T* src = phys + (size_t)plane * d.ny * L;
   {
-    constexpr int IT = NB * L / NT;  // 16: every load of the tile in flight before the first shared store
-    T re[IT], im[IT];
+    constexpr int IT = NB * L / (NT * VW);  // every load of the tile in flight before the first shared store
+    R va[IT], vb[IT];
 #pragma unroll
     for (int i = 0; i < IT; ++i) {
-      const int idx = threadIdx.x + i * NT;
-      const int p = idx / L, x = idx % L;
+      const int e = (threadIdx.x + i * NT) * VW;
+      const int p = e / L, x = e % L;
       const int ya = y0 + 2 * p, yb = ya + 1;
-      re[i] = ya < d.ny ? src[(size_t)ya * L + x] : T(0);
-      im[i] = yb < d.ny ? src[(size_t)yb * L + x] : T(0);
+      va[i] = ya < d.ny ? *reinterpret_cast<const R*>(src + (size_t)ya * L + x) : vzero<R>();
+      vb[i] = yb < d.ny ? *reinterpret_cast<const R*>(src + (size_t)yb * L + x) : vzero<R>();
     }
 #pragma unroll
     for (int i = 0; i < IT; ++i) {
-      const int idx = threadIdx.x + i * NT;
-      buf[(idx / L) * RS + sp(idx % L)] = mkc<C>(re[i], im[i]);
+      const int e = (threadIdx.x + i * NT) * VW;
+      const int p = e / L, x = e % L;
+#pragma unroll
+      for (int j = 0; j < VW; ++j) buf[p * RS + sp(x + j)] = mkc<C>(vget(va[i], j), vget(vb[i], j));
     }
   }
   __syncthreads();
@@ -384,25 +438,29 @@ __global__ void __launch_bounds__(NB * L / 16) fy_p2_kernel(TransformDims d, con
                                                            const cplx<T>* __restrict__ work,
                                                            double2* __restrict__ spec, double scale) {
   using C = cplx<T>;
-  constexpr int RS = P2<L>::RS, NT = NB * L / 16;
+  using PV = P2Vec<T>;
+  using CV = typename PV::CV;
+  constexpr int VC = PV::VC, RS = P2<L>::RS, NT = NB * L / 16;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* buf = reinterpret_cast<C*>(smem_raw);
   const int plane = blockIdx.y;
   const int k0 = blockIdx.x * NB;
   const C* src = work + (size_t)plane * d.nxh * L;
   {
-    constexpr int IT = NB * L / NT;
-    C v[IT];
+    constexpr int IT = NB * L / (NT * VC);
+    CV v[IT];
 #pragma unroll
     for (int i = 0; i < IT; ++i) {
-      const int idx = threadIdx.x + i * NT;
-      const int c = idx / L, y = idx % L;
-      v[i] = k0 + c < d.nxh ? src[(size_t)(k0 + c) * L + y] : mkc<C>(0, 0);
+      const int e = (threadIdx.x + i * NT) * VC;
+      const int c = e / L, y = e % L;
+      v[i] = k0 + c < d.nxh ? *reinterpret_cast<const CV*>(src + (size_t)(k0 + c) * L + y) : vzero<CV>();
     }
 #pragma unroll
     for (int i = 0; i < IT; ++i) {
-      const int idx = threadIdx.x + i * NT;
-      buf[(idx / L) * RS + sp(idx % L)] = v[i];
+      const int e = (threadIdx.x + i * NT) * VC;
+      const int c = e / L, y = e % L;
+#pragma unroll
+      for (int j = 0; j < VC; ++j) buf[c * RS + sp(y + j)] = cget(v[i], j);
     }
   }
   __syncthreads();
@@ -425,6 +483,7 @@ __global__ void __launch_bounds__(NB * L / 16) by_p2_kernel(TransformDims d, con
                                                            cplx<T>* __restrict__ work) {
   using C = cplx<T>;
   constexpr int RS = P2<L>::RS, NT = NB * L / 16;
+  constexpr bool RM = P2Vec<T>::kBwdRowMajor;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* buf = reinterpret_cast<C*>(smem_raw);
   const int plane = blockIdx.y;
@@ -436,31 +495,63 @@ __global__ void __launch_bounds__(NB * L / 16) by_p2_kernel(TransformDims d, con
     buf[c * RS + sp(y)] = mkc<C>(0, 0);
   }
   const double2* src = spec + (size_t)plane * d.M;
+  if constexpr (RM) {
+    // the NB columns are one contiguous run of NB*nyc coefficients; every
+    // load in flight before the first shared store
+    constexpr int IT = (NB * (L / 3 * 2) + NT - 1) / NT;  // nyc = L/3*2
+    const int run = min(NB, d.nxh - k0) * nyc;
+    const double2* s0 = src + (size_t)k0 * nyc;
+    double2 v[IT];
+#pragma unroll
+    for (int i = 0; i < IT; ++i) {
+      const int idx = threadIdx.x + i * NT;
+      v[i] = idx < run ? s0[idx] : make_double2(0.0, 0.0);
+    }
+#pragma unroll
+    for (int i = 0; i < IT; ++i) {
+      const int idx = threadIdx.x + i * NT;
+      if (idx < NB * nyc) {
+        const int c = idx / nyc, iy = idx - c * nyc;
+        buf[c * RS + sp(y_of(iy, L, nyc))] = mkc<C>((T)v[i].x, (T)v[i].y);
+      }
+    }
+  } else {
 #pragma unroll 4
-  for (int idx = threadIdx.x; idx < NB * nyc; idx += NT) {
-    const int c = idx / nyc, iy = idx - c * nyc;
-    const int k = k0 + c;
-    double2 v = k < d.nxh ? src[iy + (size_t)nyc * k] : make_double2(0.0, 0.0);
-    buf[c * RS + sp(y_of(iy, L, nyc))] = mkc<C>((T)v.x, (T)v.y);
+    for (int idx = threadIdx.x; idx < NB * nyc; idx += NT) {
+      const int c = idx / nyc, iy = idx - c * nyc;
+      const int k = k0 + c;
+      double2 v = k < d.nxh ? src[iy + (size_t)nyc * k] : make_double2(0.0, 0.0);
+      buf[c * RS + sp(y_of(iy, L, nyc))] = mkc<C>((T)v.x, (T)v.y);
+    }
   }
   __syncthreads();
   ip_passes<T, +1, L, NB, 1>(buf, tw);
   C* dst = work + (size_t)plane * d.nxh * L;
+  if constexpr (RM) {
+    // [plane][y][kx]: rows of NB kx values
 #pragma unroll 4
-  for (int idx = threadIdx.x; idx < NB * L; idx += NT) {
-    const int c = idx / L, y = idx % L;
-    if (k0 + c < d.nxh) dst[(size_t)(k0 + c) * L + y] = buf[c * RS + sp(y)];
+    for (int idx = threadIdx.x; idx < NB * L; idx += NT) {
+      const int y = idx / NB, c = idx % NB;
+      if (k0 + c < d.nxh) dst[(size_t)y * d.nxh + k0 + c] = buf[c * RS + sp(y)];
+    }
+  } else {
+    // [plane][kx][y]: NB contiguous columns
+#pragma unroll 4
+    for (int idx = threadIdx.x; idx < NB * L; idx += NT) {
+      const int c = idx / L, y = idx % L;
+      if (k0 + c < d.nxh) dst[(size_t)(k0 + c) * L + y] = buf[c * RS + sp(y)];
+    }
   }
 }
 
 // backward x pass, L = nx: two rows per complex FFT; Im of the kx = 0 coefficient ignored (c2r).
-// Each thread loads one coefficient (coalesced along y); the row pair is combined
-// across adjacent lanes.
 template <typename T, int L, int NB>
 __global__ void __launch_bounds__(NB * L / 16) bx_p2_kernel(TransformDims d, const cplx<T>* __restrict__ tw,
                                                            const cplx<T>* __restrict__ work, T* __restrict__ phys) {
   using C = cplx<T>;
-  constexpr int RS = P2<L>::RS, NT = NB * L / 16, rows = 2 * NB;
+  using PV = P2Vec<T>;
+  using R = typename PV::R;
+  constexpr int VW = PV::VW, RS = P2<L>::RS, NT = NB * L / 16, rows = 2 * NB;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* buf = reinterpret_cast<C*>(smem_raw);
   const int plane = blockIdx.y;
@@ -471,45 +562,84 @@ __global__ void __launch_bounds__(NB * L / 16) bx_p2_kernel(TransformDims d, con
     const int p = idx / gap, x = nxh + (idx - p * gap);
     buf[p * RS + sp(x)] = mkc<C>(0, 0);
   }
-  const C* src = work + (size_t)plane * nxh * d.ny;
-  const int total = rows * nxh;  // even; the pair (2p, 2p+1) sits in adjacent lanes
-  constexpr int IT = (rows * (L / 3 + 1) + NT - 1) / NT;  // nxh <= L/3 + 1
-  C hv[IT];
+  if constexpr (PV::kBwdRowMajor) {
+    // [plane][y][kx]: the 2*NB rows of the CTA are one contiguous block; each
+    // thread loads one kx of a row pair (rows 2p, 2p+1) and forms Z[k], Z[L-k]
+    const C* src = work + (size_t)plane * nxh * d.ny + (size_t)y0 * nxh;
+    const int total = NB * nxh;
+    constexpr int IT = (NB * (L / 3 + 1) + NT - 1) / NT;  // nxh <= L/3 + 1
+    C h1[IT], h2[IT];
 #pragma unroll
-  for (int i = 0; i < IT; ++i) {  // every load in flight before the pairs are combined
-    const int idx = threadIdx.x + i * NT;
-    const int k = idx / rows, q = idx % rows;
-    hv[i] = (idx < total && y0 + q < d.ny) ? src[(size_t)k * d.ny + y0 + q] : mkc<C>(0, 0);
-  }
+    for (int i = 0; i < IT; ++i) {  // every load in flight before the pairs are combined
+      const int idx = threadIdx.x + i * NT;
+      const int p = idx / nxh, k = idx - p * nxh;
+      const int ya = y0 + 2 * p;
+      h1[i] = (idx < total && ya < d.ny) ? src[(size_t)(2 * p) * nxh + k] : mkc<C>(0, 0);
+      h2[i] = (idx < total && ya + 1 < d.ny) ? src[(size_t)(2 * p + 1) * nxh + k] : mkc<C>(0, 0);
+    }
 #pragma unroll
-  for (int i = 0; i < IT; ++i) {
-    const int idx = threadIdx.x + i * NT;
-    const bool ok = idx < total;
-    const int k = idx / rows, q = idx % rows;
-    C h = hv[i];
-    if (k == 0) h.y = T(0);
-    C o;
-    o.x = __shfl_xor_sync(0xffffffffu, h.x, 1);
-    o.y = __shfl_xor_sync(0xffffffffu, h.y, 1);
-    if (ok) {
-      C* row = buf + (q >> 1) * RS;
-      if ((q & 1) == 0) {  // Z[k] = X1[k] + i X2[k], h1 = h, h2 = o
-        row[sp(k)] = mkc<C>(h.x - o.y, h.y + o.x);
-      } else if (k > 0) {  // Z[L-k] = conj(X1[k]) + i conj(X2[k]), h1 = o, h2 = h
-        row[sp(L - k)] = mkc<C>(o.x + h.y, -o.y + h.x);
+    for (int i = 0; i < IT; ++i) {
+      const int idx = threadIdx.x + i * NT;
+      if (idx < total) {
+        const int p = idx / nxh, k = idx - p * nxh;
+        C a = h1[i], b = h2[i];
+        if (k == 0) a.y = b.y = T(0);
+        C* row = buf + p * RS;
+        row[sp(k)] = mkc<C>(a.x - b.y, a.y + b.x);                  // Z[k] = X1[k] + i X2[k]
+        if (k > 0) row[sp(L - k)] = mkc<C>(a.x + b.y, -a.y + b.x);  // Z[L-k] = conj(X1[k]) + i conj(X2[k])
+      }
+    }
+  } else {
+    // [plane][kx][y]: each thread loads one coefficient (coalesced along y);
+    // the row pair is combined across adjacent lanes
+    const C* src = work + (size_t)plane * nxh * d.ny;
+    const int total = rows * nxh;  // even; the pair (2p, 2p+1) sits in adjacent lanes
+    constexpr int IT = (rows * (L / 3 + 1) + NT - 1) / NT;
+    C hv[IT];
+#pragma unroll
+    for (int i = 0; i < IT; ++i) {
+      const int idx = threadIdx.x + i * NT;
+      const int k = idx / rows, q = idx % rows;
+      hv[i] = (idx < total && y0 + q < d.ny) ? src[(size_t)k * d.ny + y0 + q] : mkc<C>(0, 0);
+    }
+#pragma unroll
+    for (int i = 0; i < IT; ++i) {
+      const int idx = threadIdx.x + i * NT;
+      const bool ok = idx < total;
+      const int k = idx / rows, q = idx % rows;
+      C h = hv[i];
+      if (k == 0) h.y = T(0);
+      C o;
+      o.x = __shfl_xor_sync(0xffffffffu, h.x, 1);
+      o.y = __shfl_xor_sync(0xffffffffu, h.y, 1);
+      if (ok) {
+        C* row = buf + (q >> 1) * RS;
+        if ((q & 1) == 0) {  // Z[k] = X1[k] + i X2[k], h1 = h, h2 = o
+          row[sp(k)] = mkc<C>(h.x - o.y, h.y + o.x);
+        } else if (k > 0) {  // Z[L-k] = conj(X1[k]) + i conj(X2[k]), h1 = o, h2 = h
+          row[sp(L - k)] = mkc<C>(o.x + h.y, -o.y + h.x);
+        }
       }
     }
   }
   __syncthreads();
   ip_passes<T, +1, L, NB, 1>(buf, tw);
   T* dst = phys + (size_t)plane * d.ny * L;
+  constexpr int IS = NB * L / (NT * VW);
 #pragma unroll 4
-  for (int idx = threadIdx.x; idx < NB * L; idx += NT) {
-    const int p = idx / L, x = idx % L;
+  for (int i = 0; i < IS; ++i) {
+    const int e = (threadIdx.x + i * NT) * VW;
+    const int p = e / L, x = e % L;
     const int ya = y0 + 2 * p, yb = ya + 1;
-    const C z = buf[p * RS + sp(x)];
-    if (ya < d.ny) dst[(size_t)ya * L + x] = z.x;
-    if (yb < d.ny) dst[(size_t)yb * L + x] = z.y;
+    R ra, rb;
+#pragma unroll
+    for (int j = 0; j < VW; ++j) {
+      const C z = buf[p * RS + sp(x + j)];
+      vset(ra, j, z.x);
+      vset(rb, j, z.y);
+    }
+    if (ya < d.ny) *reinterpret_cast<R*>(dst + (size_t)ya * L + x) = ra;
+    if (yb < d.ny) *reinterpret_cast<R*>(dst + (size_t)yb * L + x) = rb;
   }
 }
 
@@ -568,6 +698,7 @@ void fft_init() {
 }
 
 static bool p2_length(int L) { return L >= 8 && L <= 1024 && (L & (L - 1)) == 0; }
+static bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
 
 #define TG_P2_DISPATCH(L, CALL) \
   switch (L) {                  \
@@ -581,9 +712,17 @@ static bool p2_length(int L) { return L >= 8 && L <= 1024 && (L & (L - 1)) == 0;
     case 1024: CALL(1024); break; \
   }
 
-template <typename T, int L>
+// complex values per CTA of each power-of-two pass (measured at 256^2
+// planes: FP32 x and y passes 2048, the backward x pass 1024 -- smaller CTAs
+// keep more of them in flight per SM; FP64 2048 for all)
+enum P2Kind { P2_FX, P2_FY, P2_BY, P2_BX };
+template <typename T, int KIND> struct P2Elems {
+  static constexpr int value = sizeof(T) == 8 ? 2048 : KIND == P2_BX ? 1024 : 2048;
+};
+
+template <typename T, int L, int KIND>
 static size_t p2_smem() {
-  return (size_t)(P2Cta<T>::elems / L) * P2<L>::RS * sizeof(cplx<T>);
+  return (size_t)(P2Elems<T, KIND>::value / L) * P2<L>::RS * sizeof(cplx<T>);
 }
 
 template <typename T>
@@ -594,12 +733,12 @@ void dft_forward(const TransformDims& d, const FftPlan& px, const FftPlan& py, c
   {
     prof_begin(s, PC_FFT_FX, (double)planes * d.ny * (d.nx * sizeof(T) + d.nxh * sizeof(C)), 0);
     const C* tw = Tw<T>::get(px);
-    if (p2_length(px.L)) {
+    if (p2_length(px.L) && aligned16(phys)) {
 #define TG_CALL(LL)                                                                         \
   {                                                                                         \
-    constexpr int NB = P2Cta<T>::elems / LL;                                                \
+    constexpr int NB = P2Elems<T, P2_FX>::value / LL;                                                \
     dim3 grid((d.ny + 2 * NB - 1) / (2 * NB), planes);                                      \
-    fx_p2_kernel<T, LL, NB><<<grid, NB * LL / 16, p2_smem<T, LL>(), s>>>(d, tw, phys, w);   \
+    fx_p2_kernel<T, LL, NB><<<grid, NB * LL / 16, p2_smem<T, LL, P2_FX>(), s>>>(d, tw, phys, w);   \
   }
       TG_P2_DISPATCH(px.L, TG_CALL)
 #undef TG_CALL
@@ -620,9 +759,9 @@ void dft_forward(const TransformDims& d, const FftPlan& px, const FftPlan& py, c
     if (p2_length(py.L)) {
 #define TG_CALL(LL)                                                                              \
   {                                                                                              \
-    constexpr int NB = P2Cta<T>::elems / LL;                                                     \
+    constexpr int NB = P2Elems<T, P2_FY>::value / LL;                                                     \
     dim3 grid((d.nxh + NB - 1) / NB, planes);                                                    \
-    fy_p2_kernel<T, LL, NB><<<grid, NB * LL / 16, p2_smem<T, LL>(), s>>>(d, tw, w, spec, scale); \
+    fy_p2_kernel<T, LL, NB><<<grid, NB * LL / 16, p2_smem<T, LL, P2_FY>(), s>>>(d, tw, w, spec, scale); \
   }
       TG_P2_DISPATCH(py.L, TG_CALL)
 #undef TG_CALL
@@ -649,9 +788,9 @@ void dft_backward(const TransformDims& d, const FftPlan& px, const FftPlan& py, 
     if (p2_length(py.L)) {
 #define TG_CALL(LL)                                                                       \
   {                                                                                       \
-    constexpr int NB = P2Cta<T>::elems / LL;                                              \
+    constexpr int NB = P2Elems<T, P2_BY>::value / LL;                                              \
     dim3 grid((d.nxh + NB - 1) / NB, planes);                                             \
-    by_p2_kernel<T, LL, NB><<<grid, NB * LL / 16, p2_smem<T, LL>(), s>>>(d, tw, spec, w); \
+    by_p2_kernel<T, LL, NB><<<grid, NB * LL / 16, p2_smem<T, LL, P2_BY>(), s>>>(d, tw, spec, w); \
   }
       TG_P2_DISPATCH(py.L, TG_CALL)
 #undef TG_CALL
@@ -668,12 +807,12 @@ void dft_backward(const TransformDims& d, const FftPlan& px, const FftPlan& py, 
   {
     prof_begin(s, PC_FFT_BX, (double)planes * d.ny * (d.nx * sizeof(T) + d.nxh * sizeof(C)), 0);
     const C* tw = Tw<T>::get(px);
-    if (p2_length(px.L)) {
+    if (p2_length(px.L) && aligned16(phys)) {
 #define TG_CALL(LL)                                                                       \
   {                                                                                       \
-    constexpr int NB = P2Cta<T>::elems / LL;                                              \
+    constexpr int NB = P2Elems<T, P2_BX>::value / LL;                                              \
     dim3 grid((d.ny + 2 * NB - 1) / (2 * NB), planes);                                    \
-    bx_p2_kernel<T, LL, NB><<<grid, NB * LL / 16, p2_smem<T, LL>(), s>>>(d, tw, w, phys); \
+    bx_p2_kernel<T, LL, NB><<<grid, NB * LL / 16, p2_smem<T, LL, P2_BX>(), s>>>(d, tw, w, phys); \
   }
       TG_P2_DISPATCH(px.L, TG_CALL)
 #undef TG_CALL

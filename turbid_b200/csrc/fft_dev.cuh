@@ -100,11 +100,6 @@ template <int L> struct P2 {
   static constexpr int RS = L + L / 16 + 1;  // padded row stride (complex values)
 };
 
-// complex values per CTA: 4096 in FP32, 2048 in FP64 (about 35 KB of shared memory)
-template <typename T> struct P2Cta {
-  static constexpr int elems = sizeof(T) == 4 ? 4096 : 2048;
-};
-
 template <typename T, int DIR, int L, int NB, int Ns, int NT = NB * L / 16>
 __device__ __forceinline__ void ip_passes(cplx<T>* buf, const cplx<T>* __restrict__ tw, int tid = threadIdx.x) {
   using C = cplx<T>;

@@ -152,6 +152,8 @@ struct GemmArgs {
   long long out_stride;
   int M;
   int batch;          // components of this problem
+  int split;          // sym: ZOperator::split
+  double quirk;       // sym, split 2: x[n-1] += quirk * x[0]
   EpiParams ep;
 };
 
@@ -201,9 +203,11 @@ __device__ __forceinline__ void sym_store(const GemmArgs& g, int b, int r0, int 
       m[nt] = (j0 + warp * 16 + nt * 8) / 2 + (lane & 3);
       ok[nt] = m[nt] < g.M;
     }
+    // split 1: row i = P, row h+1+i = Q; otherwise row i = P + Q, row n-1-i = s (P - Q)
+    const bool sp1 = g.split == 1;
 #pragma unroll
-    for (int half = 0; half < 2; ++half) {  // row i (P + Q), then row n-1-i (s (P - Q))
-      const int r = half == 0 ? i : j;
+    for (int half = 0; half < 2; ++half) {
+      const int r = half == 0 ? i : (sp1 ? h + 1 + i : j);
       const bool row_ok = half == 0 ? i <= h : i < h;
       EpiIn in[2];
 #pragma unroll
@@ -213,7 +217,18 @@ __device__ __forceinline__ void sym_store(const GemmArgs& g, int b, int r0, int 
       for (int nt = 0; nt < 2; ++nt) {
         if (!(row_ok && ok[nt])) continue;
         const double pe = accE[mt][nt][0], pi = accE[mt][nt][1], qe = accO[mt][nt][0], qi = accO[mt][nt][1];
-        const double2 v = half == 0 ? make_double2(pe + qe, pi + qi) : make_double2(s * (pe - qe), s * (pi - qi));
+        double2 v;
+        if (sp1)
+          v = half == 0 ? make_double2(pe, pi) : make_double2(qe, qi);
+        else if (half == 0)
+          v = make_double2(pe + qe, pi + qi);
+        else {
+          v = make_double2(s * (pe - qe), s * (pi - qi));
+          if (i == 0 && g.quirk != 0.0) {  // top row after the bottom one (x[0] = P + Q)
+            v.x += g.quirk * (pe + qe);
+            v.y += g.quirk * (pi + qi);
+          }
+        }
         Cb[(size_t)r * g.M + m[nt]] = epi_apply<MODE>(g.ep, b, r, m[nt], v, in[nt]);
       }
     }
@@ -327,6 +342,7 @@ __device__ __forceinline__ void sym_body(const GemmArgs& g, const int b) {
   const int nkt = (g.K + BK - 1) / BK;
   int mt_valid = (g.rows - r0 + 7) / 8;
   mt_valid = mt_valid > MT ? MT : mt_valid;
+  const bool split_in = g.split == 2;   // input already even rows 0..h, odd rows h+1..n-1
 
   auto load_tile = [&](int kt, int buf) {
     const int k0 = kt * BK;
@@ -346,8 +362,9 @@ __device__ __forceinline__ void sym_body(const GemmArgs& g, const int b) {
       const int k = k0 + kr, j = j0 + jj;
       const bool okt = (k <= h) && (j < ncol);
       const bool okb = (k < h) && (j < ncol);
+      const int kb = split_in ? h + 1 + k : n - 1 - k;   // odd half: split rows or mirrored rows
       cp_async16(bt + kr * BST + jj, okt ? Bsrc + (size_t)k * ncol + j : Bsrc, okt);
-      cp_async16(bb + kr * BST + jj, okb ? Bsrc + (size_t)(n - 1 - k) * ncol + j : Bsrc, okb);
+      cp_async16(bb + kr * BST + jj, okb ? Bsrc + (size_t)kb * ncol + j : Bsrc, okb);
     }
   };
 
@@ -382,8 +399,8 @@ __device__ __forceinline__ void sym_body(const GemmArgs& g, const int b) {
         for (int nt = 0; nt < 2; ++nt) {
           const int bi = (ks * 4 + (lane & 3)) * BST + warp * 16 + nt * 8 + (lane >> 2);
           const double top = bt[bi], bot = bb[bi];
-          be[nt] = top + bot;
-          bo[nt] = top - bot;
+          be[nt] = split_in ? top : top + bot;
+          bo[nt] = split_in ? bot : top - bot;
         }
 #pragma unroll
         for (int mt = 0; mt < MT; ++mt) {
@@ -482,8 +499,23 @@ void row_tiling(int rows, int maxmt, int& mt, int& tiles) {
   mt = (need + tiles - 1) / tiles;
 }
 
+static void zgemm_launch(const ZProblem* probs, int nprob, int M, cudaStream_t s);
+
+// Problems of one kernel shape share a launch; a group that mixes dense and
+// folded (or split) operators runs as one launch per shape.
 void zgemm_group(const ZProblem* probs, int nprob, int M, cudaStream_t s) {
   if (nprob < 1 || nprob > kMaxGroup) throw Error{TG_ERR_ARG, "zgemm > bad group size"};
+  ZProblem part[2][kMaxGroup];
+  int np[2] = {0, 0};
+  for (int i = 0; i < nprob; ++i) {
+    const int k = probs[i].op->sym ? 1 : 0;
+    part[k][np[k]++] = probs[i];
+  }
+  for (int k = 0; k < 2; ++k)
+    if (np[k]) zgemm_launch(part[k], np[k], M, s);
+}
+
+static void zgemm_launch(const ZProblem* probs, int nprob, int M, cudaStream_t s) {
   const ZOperator& op0 = *probs[0].op;
   GemmArgs grp[kMaxGroup];
   int total = 0;
@@ -511,12 +543,16 @@ void zgemm_group(const ZProblem* probs, int nprob, int M, cudaStream_t s) {
       g.rows = op.rows;
       g.K = op.rows;
       g.sgn = op.sgn;
+      g.split = op.split;
+      g.quirk = op.quirk;
     } else {
       g.A = op.A;
       g.Ao = nullptr;
       g.rows = op.n;
       g.K = op.n;
       g.sgn = 1;
+      g.split = 0;
+      g.quirk = 0.0;
     }
     total += pr.batch;
     // flops executed (the folded product does two (h+1)^2 halves), bytes in + out + operator
@@ -583,6 +619,8 @@ void zop_build(ZOperator& op, const std::vector<double>& A, int n, bool allow_sy
     for (int j = 0; j < n; ++j) pad[(size_t)i * op.lda + j] = A[(size_t)i * n + j];
   TG_CUDA(cudaMemcpy(op.A, pad.data(), sz * sizeof(double), cudaMemcpyHostToDevice));
   op.sym = false;
+  op.split = 0;
+  op.quirk = 0.0;
   if (allow_sym && (n & 1) && n >= 5) {
     double amax = 0.0;
     for (double v : A) amax = std::max(amax, std::fabs(v));
@@ -620,6 +658,55 @@ void zop_build(ZOperator& op, const std::vector<double>& A, int n, bool allow_sy
     op.mt = op.mt_dense;
     op.tiles = op.tiles_dense;
   }
+}
+
+// One step of a split Helmholtz solve on the folded-operator kernel.
+//   split 1 (A = Einvs, rows 0..h even and h+1..n-1 odd in the column index):
+//     Ae = rows 0..h folded over the columns, Ao = rows h+1..n-1 folded;
+//     the kernel stores P at rows 0..h and Q at rows h+1..n-1.
+//   split 2 (A = Es, columns 0..h even and h+1..n-1 odd in the row index):
+//     Ae = A[0..h][0..h], Ao = A[0..h][h+1..n-1]; the kernel reads the even
+//     and odd halves of its input as they are and unfolds the output.
+void zop_build_split(ZOperator& op, const std::vector<double>& A, int n, int split, double quirk,
+                     const std::function<double*(size_t)>& alloc) {
+  if (!(n & 1) || n < 5 || (split != 1 && split != 2)) throw Error{TG_ERR_ARG, "zop_build_split > bad shape"};
+  op.n = n;
+  op.lda = (n + 15) / 16 * 16;
+  row_tiling(n, kMaxMtDense, op.mt_dense, op.tiles_dense);
+  const int h = (n - 1) / 2, hr = h + 1;
+  int mts, ts;
+  row_tiling(hr, kMaxMtSym, mts, ts);
+  const int rowsAlloc = std::max(op.tiles_dense * op.mt_dense * 8, ts * mts * 8);
+  if (op.rowsPad == 0) op.rowsPad = rowsAlloc;
+  if (op.rowsPad < rowsAlloc) throw Error{TG_ERR_ARG, "zop_build_split > operator buffer too small"};
+  const size_t sz = (size_t)op.rowsPad * op.lda;
+  if (!op.A) op.A = alloc(sz);
+  if (!op.Ae) op.Ae = alloc(sz);
+  if (!op.Ao) op.Ao = alloc(sz);
+  std::vector<double> ae(sz, 0.0), ao(sz, 0.0);
+  auto a = [&](int i, int j) { return A[(size_t)i * n + j]; };
+  if (split == 1) {
+    for (int i = 0; i < hr; ++i) {
+      for (int j = 0; j < h; ++j) ae[(size_t)i * op.lda + j] = 0.5 * (a(i, j) + a(i, n - 1 - j));
+      ae[(size_t)i * op.lda + h] = a(i, h);
+    }
+    for (int i = 0; i < h; ++i)
+      for (int j = 0; j < h; ++j) ao[(size_t)i * op.lda + j] = 0.5 * (a(h + 1 + i, j) - a(h + 1 + i, n - 1 - j));
+  } else {
+    for (int i = 0; i < hr; ++i) {
+      for (int j = 0; j < hr; ++j) ae[(size_t)i * op.lda + j] = a(i, j);
+      for (int j = 0; j < h; ++j) ao[(size_t)i * op.lda + j] = a(i, h + 1 + j);
+    }
+  }
+  TG_CUDA(cudaMemcpy(op.Ae, ae.data(), sz * sizeof(double), cudaMemcpyHostToDevice));
+  TG_CUDA(cudaMemcpy(op.Ao, ao.data(), sz * sizeof(double), cudaMemcpyHostToDevice));
+  op.sym = true;
+  op.sgn = 1;
+  op.split = split;
+  op.quirk = split == 2 ? quirk : 0.0;
+  op.rows = hr;
+  op.mt = mts;
+  op.tiles = ts;
 }
 
 }  // namespace tg

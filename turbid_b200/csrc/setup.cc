@@ -407,6 +407,60 @@ void real_eigen(const std::vector<double>& F, int n, std::vector<double>& lam, s
   }
 }
 
+// F[n-1-i][n-1-j] == F[i][j] to 1e-12 of the largest entry (odd n >= 3)
+static bool centro_symmetric(const std::vector<double>& F, int n) {
+  if (n < 3 || !(n & 1)) return false;
+  double fmax = 0.0, dev = 0.0;
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < n; ++j) {
+      fmax = std::max(fmax, std::fabs(F[(size_t)i * n + j]));
+      dev = std::max(dev, std::fabs(F[(size_t)(n - 1 - i) * n + (n - 1 - j)] - F[(size_t)i * n + j]));
+    }
+  return dev <= 1e-12 * fmax;
+}
+
+// Eigen-decomposition of a centro-symmetric F (odd n = 2m+1) from its two
+// folded halves: even vectors v[k] = v[n-1-k] = u[k] (k < m), v[m] = u[m]
+// see Fe = F[i][k] + F[i][n-1-k] (k < m), Fe[i][m] = F[i][m]; odd vectors
+// v[k] = -v[n-1-k] = u[k], v[m] = 0 see Fo = F[i][k] - F[i][n-1-k].  Columns
+// of V: the m+1 even eigenvectors, then the m odd ones; every eigenvector has
+// exact parity, which the split Helmholtz kernels rely on.
+static void folded_eigen(const std::vector<double>& F, int n, std::vector<double>& lam, std::vector<double>& V,
+                         std::vector<double>& Vinv) {
+  const int m = (n - 1) / 2, ne = m + 1, no = m;
+  std::vector<double> Fe((size_t)ne * ne), Fo((size_t)no * no);
+  for (int i = 0; i < ne; ++i) {
+    for (int k = 0; k < m; ++k) Fe[(size_t)i * ne + k] = F[(size_t)i * n + k] + F[(size_t)i * n + (n - 1 - k)];
+    Fe[(size_t)i * ne + m] = F[(size_t)i * n + m];
+  }
+  for (int i = 0; i < no; ++i)
+    for (int k = 0; k < m; ++k) Fo[(size_t)i * no + k] = F[(size_t)i * n + k] - F[(size_t)i * n + (n - 1 - k)];
+  std::vector<double> le, Ve, Vie, lo, Vo, Vio;
+  real_eigen(Fe, ne, le, Ve, Vie);
+  real_eigen(Fo, no, lo, Vo, Vio);
+  lam = le;
+  lam.insert(lam.end(), lo.begin(), lo.end());
+  V.assign((size_t)n * n, 0.0);
+  Vinv.assign((size_t)n * n, 0.0);
+  for (int j = 0; j < ne; ++j) {
+    for (int k = 0; k < m; ++k) {
+      V[(size_t)k * n + j] = V[(size_t)(n - 1 - k) * n + j] = Ve[(size_t)k * ne + j];
+      Vinv[(size_t)j * n + k] = Vinv[(size_t)j * n + (n - 1 - k)] = 0.5 * Vie[(size_t)j * ne + k];
+    }
+    V[(size_t)m * n + j] = Ve[(size_t)m * ne + j];
+    Vinv[(size_t)j * n + m] = Vie[(size_t)j * ne + m];
+  }
+  for (int j = 0; j < no; ++j) {
+    const int c = ne + j;
+    for (int k = 0; k < m; ++k) {
+      V[(size_t)k * n + c] = Vo[(size_t)k * no + j];
+      V[(size_t)(n - 1 - k) * n + c] = -Vo[(size_t)k * no + j];
+      Vinv[(size_t)c * n + k] = 0.5 * Vio[(size_t)j * no + k];
+      Vinv[(size_t)c * n + (n - 1 - k)] = -0.5 * Vio[(size_t)j * no + k];
+    }
+  }
+}
+
 void build_decomposition(int n, const std::vector<double>& D1, const std::vector<double>& D2, const double* bc,
                          Decomposition& out) {
   out.n = n;
@@ -440,7 +494,11 @@ void build_decomposition(int n, const std::vector<double>& D1, const std::vector
     for (int ix = 1; ix < n - 1; ++ix)
       F[(size_t)(ix - 1) * ni + (iz - 1)] = a(ix, iz) + a(ix, 0) * out.fbb[iz] + a(ix, n - 1) * out.ftb[iz];
   std::vector<double> lam, V, Vi;
-  real_eigen(F, ni, lam, V, Vi);
+  out.parity = centro_symmetric(F, ni);
+  if (out.parity)
+    folded_eigen(F, ni, lam, V, Vi);
+  else
+    real_eigen(F, ni, lam, V, Vi);
   out.E.assign((size_t)n * n, 0.0);
   out.Einv.assign((size_t)n * n, 0.0);
   out.lam.assign(n, 0.0);
@@ -493,6 +551,47 @@ void fold_decomposition(const Decomposition& d, bool pressure, std::vector<doubl
     Ef[j] = r0[j];
     Ef[(size_t)(n - 1) * n + j] = rn[j];
   }
+}
+
+bool split_operators(const Decomposition& d, bool pressure, std::vector<double>& Einvs, std::vector<double>& Es,
+                     double& quirk) {
+  const int n = d.n;
+  if (!d.parity || n < 5 || !(n & 1)) return false;
+  // the quirk x[n-1] += ftb[0] (x[0] - y[0]) reduces to ftb[0] x[0] only when
+  // y[0] == 0, i.e. for the pressure (boundary rows zeroed before E^-1)
+  if (!pressure && d.ftb[0] != 0.0) return false;
+  quirk = pressure ? d.ftb[0] : 0.0;
+  const int h = (n - 1) / 2;
+  std::vector<double> Ei, Ef;
+  fold_decomposition(d, pressure, Ei, Ef);
+  for (int j = 0; j < n; ++j) {  // row N-1 := ftb . E with E's own row 0 (the quirk is applied by the kernel)
+    double s = 0.0;
+    for (int k = 0; k < n; ++k) s += d.ftb[k] * d.E[(size_t)k * n + j];
+    Ef[(size_t)(n - 1) * n + j] = s;
+  }
+  Einvs = Ei;
+  Es = Ef;
+  for (int j = 0; j < n; ++j) {
+    const double r0 = Ei[j], rn = Ei[(size_t)(n - 1) * n + j];
+    Einvs[j] = r0 + rn;
+    Einvs[(size_t)(n - 1) * n + j] = r0 - rn;
+    const double c0 = Ef[(size_t)j * n], cn = Ef[(size_t)j * n + n - 1];
+    Es[(size_t)j * n] = 0.5 * (c0 + cn);
+    Es[(size_t)j * n + n - 1] = 0.5 * (c0 - cn);
+  }
+  if (pressure)  // y'0 = y'N = 0 (rows 0, N-1 of Einvs vanish): the boundary columns multiply zeros
+    for (int i = 0; i < n; ++i) Es[(size_t)i * n] = Es[(size_t)i * n + n - 1] = 0.0;
+  // parity of the rows of Einvs and of the columns of Es (even block 0..h)
+  double ai = 0.0, ae = 0.0, di = 0.0, de = 0.0;
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < n; ++j) {
+      const double sg = (i <= h) ? 1.0 : -1.0, sc = (j <= h) ? 1.0 : -1.0;
+      ai = std::max(ai, std::fabs(Einvs[(size_t)i * n + j]));
+      ae = std::max(ae, std::fabs(Es[(size_t)i * n + j]));
+      di = std::max(di, std::fabs(Einvs[(size_t)i * n + (n - 1 - j)] - sg * Einvs[(size_t)i * n + j]));
+      de = std::max(de, std::fabs(Es[(size_t)(n - 1 - i) * n + j] - sc * Es[(size_t)i * n + j]));
+    }
+  return di <= 1e-11 * ai && de <= 1e-11 * ae;
 }
 
 }  // namespace tg

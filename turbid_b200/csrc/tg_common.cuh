@@ -159,6 +159,12 @@ struct ZOperator {
   int n = 0, lda = 0, rowsPad = 0;
   bool sym = false;
   int sgn = 1;
+  // split solve halves (sym kernel): 0 = folded input and output of a
+  // centro-(anti)symmetric operator; 1 = folded input, output rows 0..h the
+  // even products and h+1..n-1 the odd ones; 2 = that split input, unfolded
+  // output, plus x[n-1] += quirk * x[0]
+  int split = 0;
+  double quirk = 0.0;
   int rows = 0, mt = 0, tiles = 0;       // launch shape of the kernel used
   int mt_dense = 0, tiles_dense = 0;
   double* A = nullptr;
@@ -182,6 +188,9 @@ void zgemm_init();
 void row_tiling(int rows, int maxmt, int& mt, int& tiles);
 void zop_build(ZOperator& op, const std::vector<double>& A, int n, bool allow_sym,
                const std::function<double*(size_t)>& alloc);
+// halves of one step of a split Helmholtz solve (split = 1: Einvs, 2: Es)
+void zop_build_split(ZOperator& op, const std::vector<double>& A, int n, int split, double quirk,
+                     const std::function<double*(size_t)>& alloc);
 void zgemm(const ZOperator& op, const double2* in, long long in_stride, double2* out, long long out_stride, int M,
            int batch, const EpiParams& ep, cudaStream_t s);
 // up to three problems whose operators share the kernel shape, in one launch
