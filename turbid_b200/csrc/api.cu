@@ -121,6 +121,12 @@ struct Ctx {
   bool overlap = true, overlap_active = false, sc_pending = false;
   cudaStream_t s2 = nullptr;
   cudaEvent_t cc_done = nullptr, sc_done = nullptr;
+  // The w solve of the carrier Predict, when it is split (folded kernel), runs
+  // on a third stream beside the u and v solves (dense kernel), so that the
+  // two launches fill each other's tails; same conditions as the overlap.
+  bool fork_active = false;
+  cudaStream_t s3 = nullptr;
+  cudaEvent_t w_fork = nullptr, w_join = nullptr;
   double2 *TMP_s = nullptr, *F6_s = nullptr;
   void *PRD_s = nullptr, *DUP_s = nullptr, *work_s = nullptr, *PLN2 = nullptr, *PLN1 = nullptr;
   std::vector<void*> allocs;
@@ -146,8 +152,11 @@ struct Ctx {
     if (s2) cudaStreamDestroy(s2);
     if (cc_done) cudaEventDestroy(cc_done);
     if (sc_done) cudaEventDestroy(sc_done);
-    s2 = nullptr;
-    cc_done = sc_done = nullptr;
+    if (s3) cudaStreamDestroy(s3);
+    if (w_fork) cudaEventDestroy(w_fork);
+    if (w_join) cudaEventDestroy(w_join);
+    s2 = s3 = nullptr;
+    cc_done = sc_done = w_fork = w_join = nullptr;
   }
   void drop_graphs() {
     for (auto& g : gexec) {
@@ -378,6 +387,9 @@ static Ctx* create(const tg_case& c) {
   std::memset(x.force_h, 0, 4 * sizeof(double));
   TG_CUDA(cudaEventCreateWithFlags(&x.fev[0], cudaEventDisableTiming));
   TG_CUDA(cudaEventCreateWithFlags(&x.fev[1], cudaEventDisableTiming));
+  TG_CUDA(cudaStreamCreateWithFlags(&x.s3, cudaStreamNonBlocking));
+  TG_CUDA(cudaEventCreateWithFlags(&x.w_fork, cudaEventDisableTiming));
+  TG_CUDA(cudaEventCreateWithFlags(&x.w_join, cudaEventDisableTiming));
   return px.release();
 }
 
@@ -573,8 +585,19 @@ static void carrier_predict(Ctx& x, int stage) {
       fwd[i] = ZProblem{&x.opEinv[i], x.RHS + i * S, (long long)S, x.TMP + i * S, (long long)S, 1, ep};
       bwd[i] = ZProblem{&x.opE[i], x.TMP + i * S, (long long)S, x.SU + i * S, (long long)S, 1, EpiParams()};
     }
-    zgemm_group(fwd, 3, x.M, x.s);
-    zgemm_group(bwd, 3, x.M, x.s);
+    if (x.fork_active && x.opEinv[2].sym && x.opE[2].sym) {
+      TG_CUDA(cudaEventRecord(x.w_fork, x.s));
+      TG_CUDA(cudaStreamWaitEvent(x.s3, x.w_fork, 0));
+      zgemm_group(&fwd[2], 1, x.M, x.s3);
+      zgemm_group(&bwd[2], 1, x.M, x.s3);
+      TG_CUDA(cudaEventRecord(x.w_join, x.s3));
+      zgemm_group(fwd, 2, x.M, x.s);
+      zgemm_group(bwd, 2, x.M, x.s);
+      TG_CUDA(cudaStreamWaitEvent(x.s, x.w_join, 0));
+    } else {
+      zgemm_group(fwd, 3, x.M, x.s);
+      zgemm_group(bwd, 3, x.M, x.s);
+    }
   }
 }
 
@@ -838,16 +861,17 @@ static bool graph_eligible(const Ctx& x) {
 template <typename T>
 static void record_step(Ctx& x) {
   x.overlap_active = x.overlap && x.scalar && !g_prof;  // profiled steps run sequentially
+  x.fork_active = x.overlap && !g_prof;
   try {
     for (int st = 0; st < 3; ++st) run_stage<T>(x, st);
     join_scalar(x);  // a captured step ends joined
   } catch (...) {
-    x.overlap_active = false;
+    x.overlap_active = x.fork_active = false;
     x.sc_pending = false;
     x.PLN = x.PLN1;
     throw;
   }
-  x.overlap_active = false;
+  x.overlap_active = x.fork_active = false;
 }
 
 static void run_step_graph(Ctx& x) {
@@ -912,6 +936,7 @@ static void enqueue_step(Ctx& x, int slot) {
     run_step_graph(x);
   } else {
     x.overlap_active = x.overlap && x.scalar && !g_prof;  // profiled steps run sequentially
+    x.fork_active = x.overlap && !g_prof;
     try {
       if (x.mixed)
         for (int st = 0; st < 3; ++st) run_stage<float>(x, st);
@@ -919,10 +944,10 @@ static void enqueue_step(Ctx& x, int slot) {
         for (int st = 0; st < 3; ++st) run_stage<double>(x, st);
       join_scalar(x);
     } catch (...) {
-      x.overlap_active = false;
+      x.overlap_active = x.fork_active = false;
       throw;
     }
-    x.overlap_active = false;
+    x.overlap_active = x.fork_active = false;
   }
   x.alternation = !x.alternation;
   TG_CUDA(cudaMemcpyAsync(x.feat_h + slot * 100, x.feat, 100 * sizeof(double), cudaMemcpyDeviceToHost, x.s));

@@ -325,7 +325,7 @@ __device__ __forceinline__ void dense_body(const GemmArgs& g, const int b) {
 // ---------------------------------------------------------------------------
 // sym: folded rows [r0, r0 + 8*MT) of P and Q, columns [j0, j0 + 128) reals
 // ---------------------------------------------------------------------------
-template <int MT>
+template <int MT, bool SPLIT_IN>
 __device__ __forceinline__ void sym_body(const GemmArgs& g, const int b) {
   constexpr int BM = 8 * MT, BN = 128, BST = BN + 4;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -342,7 +342,7 @@ __device__ __forceinline__ void sym_body(const GemmArgs& g, const int b) {
   const int nkt = (g.K + BK - 1) / BK;
   int mt_valid = (g.rows - r0 + 7) / 8;
   mt_valid = mt_valid > MT ? MT : mt_valid;
-  const bool split_in = g.split == 2;   // input already even rows 0..h, odd rows h+1..n-1
+  constexpr bool split_in = SPLIT_IN;   // input already even rows 0..h, odd rows h+1..n-1 (split 2)
 
   auto load_tile = [&](int kt, int buf) {
     const int k0 = kt * BK;
@@ -452,9 +452,9 @@ __global__ void __launch_bounds__(kThreads) zgemm_dense_kernel(GemmArgs g0, Gemm
 #undef TG_BODY
 }
 
-template <int MT, int NP>
+template <int MT, int NP, bool SPLIT_IN>
 __global__ void __launch_bounds__(kThreads, 2) zgemm_sym_kernel(GemmArgs g0, GemmArgs g1, GemmArgs g2) {
-#define TG_BODY(G, Z) sym_body<MT>(G, Z)
+#define TG_BODY(G, Z) sym_body<MT, SPLIT_IN>(G, Z)
   TG_GROUP_DISPATCH(TG_BODY)
 #undef TG_BODY
 }
@@ -482,13 +482,17 @@ void zgemm_init() {
                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dense_smem<MT>()));
   TG_MT_LIST(TG_SET)
 #undef TG_SET
-#define TG_SET(MT)                                                                                           \
-  TG_CUDA(cudaFuncSetAttribute(zgemm_sym_kernel<MT, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,        \
-                               (int)sym_smem<MT>()));                                                        \
-  TG_CUDA(cudaFuncSetAttribute(zgemm_sym_kernel<MT, kMaxGroup>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+#define TG_SET_ONE(MT, NP, SI)                                                                           \
+  TG_CUDA(cudaFuncSetAttribute(zgemm_sym_kernel<MT, NP, SI>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
                                (int)sym_smem<MT>()));
+#define TG_SET(MT)                      \
+  TG_SET_ONE(MT, 1, false)              \
+  TG_SET_ONE(MT, kMaxGroup, false)      \
+  TG_SET_ONE(MT, 1, true)               \
+  TG_SET_ONE(MT, kMaxGroup, true)
   TG_MT_SYM_LIST(TG_SET)
 #undef TG_SET
+#undef TG_SET_ONE
 }
 
 // m-tiles per CTA for `rows` rows: as few row tiles as possible with at most
@@ -501,17 +505,18 @@ void row_tiling(int rows, int maxmt, int& mt, int& tiles) {
 
 static void zgemm_launch(const ZProblem* probs, int nprob, int M, cudaStream_t s);
 
-// Problems of one kernel shape share a launch; a group that mixes dense and
-// folded (or split) operators runs as one launch per shape.
+// Problems of one kernel shape share a launch; a group that mixes dense,
+// folded and split-input operators runs as one launch per shape.
 void zgemm_group(const ZProblem* probs, int nprob, int M, cudaStream_t s) {
   if (nprob < 1 || nprob > kMaxGroup) throw Error{TG_ERR_ARG, "zgemm > bad group size"};
-  ZProblem part[2][kMaxGroup];
-  int np[2] = {0, 0};
+  ZProblem part[3][kMaxGroup];
+  int np[3] = {0, 0, 0};
   for (int i = 0; i < nprob; ++i) {
-    const int k = probs[i].op->sym ? 1 : 0;
+    const ZOperator& op = *probs[i].op;
+    const int k = !op.sym ? 0 : (op.split == 2 ? 2 : 1);
     part[k][np[k]++] = probs[i];
   }
-  for (int k = 0; k < 2; ++k)
+  for (int k = 0; k < 3; ++k)
     if (np[k]) zgemm_launch(part[k], np[k], M, s);
 }
 
@@ -523,7 +528,8 @@ static void zgemm_launch(const ZProblem* probs, int nprob, int M, cudaStream_t s
   for (int i = 0; i < nprob; ++i) {
     const ZProblem& pr = probs[i];
     const ZOperator& op = *pr.op;
-    if (op.sym != op0.sym || op.mt != op0.mt || op.tiles != op0.tiles || op.n != op0.n)
+    if (op.sym != op0.sym || op.mt != op0.mt || op.tiles != op0.tiles || op.n != op0.n ||
+        (op.split == 2) != (op0.split == 2))
       throw Error{TG_ERR_ARG, "zgemm > operators of one launch differ in shape"};
     GemmArgs& g = grp[i];
     g.lda = op.lda;
@@ -565,16 +571,19 @@ static void zgemm_launch(const ZProblem* probs, int nprob, int M, cudaStream_t s
   }
   prof_begin(s, PC_GEMM, by, fl);
   if (op0.sym) {
+    const bool split_in = op0.split == 2;
     dim3 grid(op0.tiles, (2 * M + 127) / 128, total);
-#define TG_CASE(MT)                                                                                     \
-  case MT:                                                                                              \
-    if (nprob == 1)                                                                                     \
-      zgemm_sym_kernel<MT, 1><<<grid, kThreads, sym_smem<MT>(), s>>>(grp[0], grp[1], grp[2]);          \
-    else                                                                                                \
-      zgemm_sym_kernel<MT, kMaxGroup><<<grid, kThreads, sym_smem<MT>(), s>>>(grp[0], grp[1], grp[2]);  \
+#define TG_SYM(MT, NP, SI) zgemm_sym_kernel<MT, NP, SI><<<grid, kThreads, sym_smem<MT>(), s>>>(grp[0], grp[1], grp[2])
+#define TG_CASE(MT)                                              \
+  case MT:                                                       \
+    if (nprob == 1)                                              \
+      split_in ? TG_SYM(MT, 1, true) : TG_SYM(MT, 1, false);     \
+    else                                                         \
+      split_in ? TG_SYM(MT, kMaxGroup, true) : TG_SYM(MT, kMaxGroup, false); \
     break;
     switch (op0.mt) { TG_MT_SYM_LIST(TG_CASE) default: throw Error{TG_ERR_ARG, "zgemm > bad tiling"}; }
 #undef TG_CASE
+#undef TG_SYM
   } else {
     dim3 grid(op0.tiles, (2 * M + 127) / 128, total);
 #define TG_CASE(MT)                                                                                       \
