@@ -404,58 +404,86 @@ void erosion_row(double2* rhs, const double2* ero, const double2* phi, int M, do
 }
 
 // --- Bartnicki positivity filter (phase_scalar_flat.cc:419-478) -----------------
-// One CTA per z plane: per-plane sums of positive, zero and negative values and
-// their counts, then the redistribution; five sweeps in one launch.
-template <typename T>
-__global__ void __launch_bounds__(1024) k_filter(T* __restrict__ phip, int plane_n) {
-  __shared__ double red[6][32];
-  __shared__ double tot[6];
-  T* p = phip + (size_t)blockIdx.x * plane_n;
+// One CTA per z plane, five sweeps in one launch.  Each sweep needs the sums
+// of the positive and the negative values of the plane and their counts (the
+// zero class sums to zero); the redistribution of sweep k and the sums for
+// sweep k+1 share one pass over the plane, which stays in L2.  Passes run in
+// batches of FB values per thread, all loads of a batch in flight together.
+constexpr int kFilterThreads = 1024, kFilterBatch = 8;
+
+__device__ __forceinline__ void filter_reduce(double (&a)[4], double (*red)[32], double* tot) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  for (int it = 0; it < 5; ++it) {
-    double a[6] = {0, 0, 0, 0, 0, 0};
-    for (int i = threadIdx.x; i < plane_n; i += blockDim.x) {
-      double v = (double)p[i];
-      if (v > 0) {
-        a[0] += v;
-        a[1] += 1;
-      } else if (v < 0) {
-        a[4] += v;
-        a[5] += 1;
-      } else {
-        a[2] += v;
-        a[3] += 1;
-      }
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    double x = a[k];
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+    if (lane == 0) red[k][warp] = x;
+  }
+  __syncthreads();
+  if (threadIdx.x < 4) {
+    double x = 0;
+    for (int w = 0; w < nw; ++w) x += red[threadIdx.x][w];
+    tot[threadIdx.x] = x;
+  }
+  __syncthreads();
+}
+
+template <typename T>
+__device__ __forceinline__ void filter_classify(T x, double& sp, int& cp, double& sn, int& cn) {
+  const double d = (double)x;
+  sp += d > 0 ? d : 0.0;
+  cp += d > 0 ? 1 : 0;
+  sn += d < 0 ? d : 0.0;
+  cn += d < 0 ? 1 : 0;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kFilterThreads, 2) k_filter(T* __restrict__ phip, int plane_n) {
+  constexpr int FB = kFilterBatch, STEP = FB * kFilterThreads;
+  __shared__ double red[4][32];
+  __shared__ double tot[4];
+  T* p = phip + (size_t)blockIdx.x * plane_n;
+  double sp = 0, sn = 0;
+  int cp = 0, cn = 0;
+  for (int i0 = threadIdx.x; i0 < plane_n; i0 += STEP) {
+    T x[FB];
+#pragma unroll
+    for (int b = 0; b < FB; ++b) {
+      const int i = i0 + b * kFilterThreads;
+      x[b] = i < plane_n ? p[i] : T(0);
     }
 #pragma unroll
-    for (int k = 0; k < 6; ++k) {
-      double v = a[k];
-      for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-      if (lane == 0) red[k][warp] = v;
+    for (int b = 0; b < FB; ++b) filter_classify(x[b], sp, cp, sn, cn);
+  }
+  for (int it = 0; it < 5; ++it) {
+    double a[4] = {sp, (double)cp, sn, (double)cn};
+    filter_reduce(a, red, tot);
+    const bool kill = (tot[0] + tot[2]) < 0;
+    const double add = tot[1] > 0 ? tot[2] / tot[1] : 0.0;
+    sp = sn = 0;
+    cp = cn = 0;
+    for (int i0 = threadIdx.x; i0 < plane_n; i0 += STEP) {
+      T x[FB];
+#pragma unroll
+      for (int b = 0; b < FB; ++b) {
+        const int i = i0 + b * kFilterThreads;
+        x[b] = i < plane_n ? p[i] : T(0);
+      }
+#pragma unroll
+      for (int b = 0; b < FB; ++b) {
+        const int i = i0 + b * kFilterThreads;
+        const T y = kill ? T(0) : ((x[b] > 0) ? (T)((double)x[b] + add) : T(0));
+        if (i < plane_n) p[i] = y;
+        filter_classify(y, sp, cp, sn, cn);   // sums for the next sweep
+      }
     }
-    __syncthreads();
-    if (threadIdx.x < 6) {
-      double s = 0;
-      for (int w = 0; w < nw; ++w) s += red[threadIdx.x][w];
-      tot[threadIdx.x] = s;
-    }
-    __syncthreads();
-    const bool kill = (tot[0] + tot[2] + tot[4]) < 0;
-    const double add = tot[1] > 0 ? tot[4] / tot[1] : 0.0;
-    for (int i = threadIdx.x; i < plane_n; i += blockDim.x) {
-      T v = p[i];
-      if (kill)
-        p[i] = T(0);
-      else
-        p[i] = (v > 0) ? (T)((double)v + add) : T(0);
-    }
-    __syncthreads();
+    __syncthreads();   // the next sweep's reduction reuses red/tot
   }
 }
 template <typename T>
 void positivity_filter(T* phip, int plane_n, int nz, cudaStream_t s) {
-  prof_begin(s, PC_FILTER, 20.0 * sizeof(T) * (double)plane_n * nz, 0);
-  k_filter<T><<<nz, 1024, 0, s>>>(phip, plane_n);
+  prof_begin(s, PC_FILTER, 11.0 * sizeof(T) * (double)plane_n * nz, 0);   // 6 reads + 5 writes of the plane
+  k_filter<T><<<nz, kFilterThreads, 0, s>>>(phip, plane_n);
   prof_end(s);
   TG_LAUNCH_CHECK("k_filter");
 }
