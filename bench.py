@@ -430,8 +430,12 @@ def our_arm(args):
     elif dom == "zgemm":
         peak = fp64_gemm_peak(torch)
         achieved = d["flops"] / (d["ms"] * 1e-3) / 1e12
-        roof = {"kernel": "zgemm_dense_kernel / zgemm_sym_kernel (FP64 DMMA z-operator GEMM; flops executed)", "bound": "tensor", "achieved": achieved,
-                "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+        executed = d.get("xflops", d["flops"]) / (d["ms"] * 1e-3) / 1e12
+        roof = {"kernel": "zgemm_dense_kernel / zgemm_sym_kernel (FP64 DMMA z-operator GEMMs)", "bound": "tensor",
+                "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                "flops": "algorithmic: 4 Nz^2 M per component application (the dense product the reference "
+                         "performs); the folded and split kernels execute about half of that",
+                "executed_tflops": executed, "executed_frac": executed / peak,
                 "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no FP64 figure)",
                 "per_launch_flops": d["flops"] / max(d["count"], 1), "traffic": traffic}
     else:
@@ -450,6 +454,7 @@ def our_arm(args):
                "hbm_frac": gbs / hbm}
         if v["flops"]:
             ent["TFLOP/s"] = v["flops"] / (v["ms"] * 1e-3) / 1e12
+            ent["executed_TFLOP/s"] = v.get("xflops", v["flops"]) / (v["ms"] * 1e-3) / 1e12
         kernels[k] = ent
 
     cpu = None

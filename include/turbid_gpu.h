@@ -193,11 +193,15 @@ TG_API tg_status tg_features(tg_ctx* ctx, double* out);
  * class the summed device milliseconds, algorithmic bytes and flops and the
  * launch count.  Classes: 0 z-operator GEMM, 1 forward x pass, 2 forward y
  * pass, 3 backward y pass, 4 backward x pass, 5 elementwise, 6 positivity
- * filter, 7 feature reduction. */
+ * filter, 7 feature reduction.  The algorithmic flops of a z-operator are
+ * those of the dense product, 4 Nz^2 M per component (the reference's count);
+ * tg_profile_executed returns, for the window that tg_profile_end closed, the
+ * flops the kernels executed (half of those for folded or split operators). */
 #define TG_PROF_NCAT 8
 TG_API tg_status tg_profile_begin(tg_ctx* ctx);
 TG_API tg_status tg_profile_end(tg_ctx* ctx, int ncat, double* ms, double* bytes,
                                 double* flops, int* count);
+TG_API tg_status tg_profile_executed(const tg_ctx* ctx, int ncat, double* flops);
 
 /* Field-container primitives on device buffers (layouts above). */
 /* RealCplxCube::DftForward (src/cube_real_cplx.cc:525-539): pruned x r2c,

@@ -95,6 +95,7 @@ _SIGS = [
     ("tg_features", _c_i, [_vp, _pd]),
     ("tg_profile_begin", _c_i, [_vp]),
     ("tg_profile_end", _c_i, [_vp, _c_i, _pd, _pd, _pd, _pi]),
+    ("tg_profile_executed", _c_i, [_vp, _c_i, _pd]),
     ("tg_dft_forward_f64", _c_i, [_vp, _vp, _vp, _c_i]),
     ("tg_dft_forward_f32", _c_i, [_vp, _vp, _vp, _c_i]),
     ("tg_dft_forward_f64_noalloc", _c_i, [_c_i, _c_i, _c_i, _vp, _vp, _c_i, _vp]),

@@ -39,10 +39,11 @@ void fft_init();
 struct Profiler {
   struct Rec {
     int cat;
-    double bytes, flops;
+    double bytes, flops, xflops;
     cudaEvent_t a, b;
   };
   std::vector<Rec> recs;
+  double last_x[TG_PROF_NCAT] = {0};  // executed flops of the window tg_profile_end closed
   std::vector<cudaEvent_t> pool;
   size_t used = 0;
   cudaEvent_t get() {
@@ -63,9 +64,9 @@ struct Profiler {
 };
 thread_local Profiler* g_prof = nullptr;
 
-void prof_begin(cudaStream_t s, int cat, double bytes, double flops) {
+void prof_begin(cudaStream_t s, int cat, double bytes, double flops, double xflops) {
   if (!g_prof) return;
-  Profiler::Rec r{cat, bytes, flops, g_prof->get(), g_prof->get()};
+  Profiler::Rec r{cat, bytes, flops, xflops < 0 ? flops : xflops, g_prof->get(), g_prof->get()};
   TG_CUDA(cudaEventRecord(r.a, s));
   g_prof->recs.push_back(r);
 }
@@ -1383,7 +1384,9 @@ tg_status tg_profile_end(tg_ctx* ctx, int ncat, double* ms, double* bytes, doubl
       if (flops) flops[c] = 0;
       if (count) count[c] = 0;
     }
+    for (double& v : x.prof.last_x) v = 0.0;
     for (auto& r : x.prof.recs) {
+      if (r.cat >= 0 && r.cat < TG_PROF_NCAT) x.prof.last_x[r.cat] += r.xflops;
       if (r.cat < 0 || r.cat >= ncat) continue;
       float t = 0.f;
       TG_CUDA(cudaEventElapsedTime(&t, r.a, r.b));
@@ -1394,6 +1397,17 @@ tg_status tg_profile_end(tg_ctx* ctx, int ncat, double* ms, double* bytes, doubl
     }
     x.prof.reset();
   });
+}
+
+tg_status tg_profile_executed(const tg_ctx* ctx, int ncat, double* flops) {
+  TG_CHECK_CTX(ctx);
+  const Ctx& x = *reinterpret_cast<const Ctx*>(ctx);
+  if (!flops || ncat < 0) {
+    set_error("tg_profile_executed > bad argument");
+    return TG_ERR_ARG;
+  }
+  for (int c = 0; c < ncat; ++c) flops[c] = c < TG_PROF_NCAT ? x.prof.last_x[c] : 0.0;
+  return TG_OK;
 }
 
 tg_status tg_features(tg_ctx* ctx, double* out) {

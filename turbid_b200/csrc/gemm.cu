@@ -524,7 +524,7 @@ static void zgemm_launch(const ZProblem* probs, int nprob, int M, cudaStream_t s
   const ZOperator& op0 = *probs[0].op;
   GemmArgs grp[kMaxGroup];
   int total = 0;
-  double fl = 0.0, by = 0.0;
+  double fl = 0.0, xfl = 0.0, by = 0.0;
   for (int i = 0; i < nprob; ++i) {
     const ZProblem& pr = probs[i];
     const ZOperator& op = *pr.op;
@@ -562,14 +562,15 @@ static void zgemm_launch(const ZProblem* probs, int nprob, int M, cudaStream_t s
     }
     total += pr.batch;
     // flops executed (the folded product does two (h+1)^2 halves), bytes in + out + operator
-    fl += (op.sym ? 2.0 * 4.0 * op.rows * op.rows : 4.0 * op.n * op.n) * (double)M * pr.batch;
+    fl += 4.0 * op.n * op.n * (double)M * pr.batch;   // algorithmic: the dense product
+    xfl += (op.sym ? 2.0 * 4.0 * op.rows * op.rows : 4.0 * op.n * op.n) * (double)M * pr.batch;
     by += (double)pr.batch * 16.0 * M * 2 * op.n + 8.0 * op.n * op.n;
   }
   for (int i = nprob; i < kMaxGroup; ++i) {
     grp[i] = grp[0];
     grp[i].batch = 0;
   }
-  prof_begin(s, PC_GEMM, by, fl);
+  prof_begin(s, PC_GEMM, by, fl, xfl);
   if (op0.sym) {
     const bool split_in = op0.split == 2;
     dim3 grid(op0.tiles, (2 * M + 127) / 128, total);

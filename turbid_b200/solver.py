@@ -138,7 +138,10 @@ class ChannelCase:
         ms, by, fl = (np.zeros(n) for _ in range(3))
         cnt = np.zeros(n, dtype=np.int32)
         check(self.lib.tg_profile_end(self.h, n, _p(ms), _p(by), _p(fl), cnt.ctypes.data_as(ctypes.POINTER(ctypes.c_int))))
-        return {name: dict(ms=float(ms[i]), bytes=float(by[i]), flops=float(fl[i]), count=int(cnt[i]))
+        xf = np.zeros(n)
+        check(self.lib.tg_profile_executed(self.h, n, _p(xf)))
+        return {name: dict(ms=float(ms[i]), bytes=float(by[i]), flops=float(fl[i]), xflops=float(xf[i]),
+                           count=int(cnt[i]))
                 for i, name in enumerate(_lib.PROF_NAMES)}
 
     # ---- plugin methods
