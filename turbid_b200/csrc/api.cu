@@ -421,6 +421,28 @@ static void bwd(Ctx& x, const double2* spec, void* phys, int planes) {
   }
 }
 
+// Backward transforms of nf fields gathered from their own spectral sources,
+// the x and y derivatives (deriv 1, 2) formed as the coefficients are loaded:
+// the spectral derivative fields are never written.
+template <typename T>
+static void bwd_gather(Ctx& x, const double2* const* src, const int* deriv, int nf, void* phys) {
+  if (nf < 1 || nf > kMaxGather) throw Error{TG_ERR_ARG, "bwd_gather > bad field count"};
+  SpecGather g{};
+  for (int f = 0; f < nf; ++f) {
+    g.src[f] = src[f];
+    g.deriv[f] = deriv[f];
+  }
+  g.kx = x.kx;
+  g.ky = x.ky;
+  g.nf = nf;
+  const int planes = nf * x.nz;
+  for (int p0 = 0; p0 < planes; p0 += x.work_planes) {
+    const int np = std::min(planes - p0, x.work_planes);
+    g.plane0 = p0;
+    dft_backward<T>(x.td, x.px, x.py, nullptr, (T*)phys + (size_t)p0 * x.nx * x.ny, np, x.work, x.s, &g);
+  }
+}
+
 // driving force of the mean mode (src/phase_carrier_flat.cc:365-501)
 static void mean_force(const Ctx& x, double& f1, double& f2) {
   const tg_case& c = x.c;
@@ -473,17 +495,8 @@ static void carrier_predict(Ctx& x, int stage) {
   T* unl = (T*)x.UNL;
   T* prd = (T*)x.PRD;
   T* dup = (T*)x.DUP;
-  auto grad_u = [&]() {  // SpaceStepper::Gradient(uvw, d*dxyz, i) for i = 0..2
-    EpiParams ep;
-    ep.mode = EPI_GRAD;
-    ep.kx = x.kx;
-    ep.ky = x.ky;
-    ep.X0 = x.U;
-    ep.sX = S;
-    ep.aux0 = x.DU;
-    ep.aux1 = x.DU + S;
-    ep.sAux = 3 * S;
-    gemm(x, x.opD1, x.U, S, x.DU + 2 * S, 3 * S, 3, ep);
+  auto grad_u = [&]() {  // SpaceStepper::Gradient(uvw, d*dxyz, i) for i = 0..2: d/dz here, d/dx and d/dy
+    gemm(x, x.opD1, x.U, S, x.DU + 2 * S, 3 * S, 3, EpiParams());   // are formed by the transform's loads
   };
   // NonlinearVelocity (phase_carrier_flat.cc:716-813)
   if (x.alternation) {
@@ -507,7 +520,16 @@ static void carrier_predict(Ctx& x, int stage) {
     wall_dz(x.U, x.DU, S, x.M, x.nz, x.d1r0, x.d1rn, x.s);
   } else {
     grad_u();
-    bwd<T>(x, x.DU, dup, 9 * x.nz);
+    const double2* src[9];
+    int der[9];
+    for (int i = 0; i < 3; ++i) {  // field 3i+j: d u_i / d x_j
+      src[3 * i + 0] = src[3 * i + 1] = x.U + i * S;
+      der[3 * i + 0] = 1;
+      der[3 * i + 1] = 2;
+      src[3 * i + 2] = x.DU + (3 * i + 2) * S;
+      der[3 * i + 2] = 0;
+    }
+    bwd_gather<T>(x, src, der, 9, dup);
     adv_products<T>(unl, dup, prd, P, 3, 0.0, 0.0, 0.0, x.s);
     fwd<T>(x, prd, x.ADV, 3 * x.nz);
   }
@@ -629,19 +651,12 @@ static void carrier_correct(Ctx& x, int stage) {
     gemm(x, x.opEinv[3], x.TMP, S, x.TMP + S, S, 1, ep);
     gemm(x, x.opE[3], x.TMP + S, S, x.PR, S, 1, EpiParams());
   }
-  {  // grad p (phase_carrier_flat.cc:597)
-    EpiParams ep;
-    ep.mode = EPI_GRAD;
-    ep.kx = x.kx;
-    ep.ky = x.ky;
-    ep.X0 = x.PR;
-    ep.aux0 = x.DP;
-    ep.aux1 = x.DP + S;
-    gemm(x, x.opD1, x.PR, S, x.DP + 2 * S, S, 1, ep);
-  }
+  // grad p (phase_carrier_flat.cc:597): dp/dz here; dp/dx, dp/dy = i kx p, i ky p
+  // are formed from p by the two kernels that read them
+  gemm(x, x.opD1, x.PR, S, x.DP + 2 * S, S, 1, EpiParams());
   if (stage == 2) x.olddt = dt;   // boundary_carrier_flat.cc:140-142
-  boundary_update(x.hist, x.DP, S, x.M, x.nz, x.opentop ? 1 : 0, x.kx, x.ky, x.d1r0, x.d1rn, x.s);
-  project(x.U, x.SU, x.DP, S, x.M, 2 * dt * c3, x.s);
+  boundary_update(x.hist, x.PR, x.DP + 2 * S, x.M, x.nz, x.opentop ? 1 : 0, x.kx, x.ky, x.d1r0, x.d1rn, x.s);
+  project(x.U, x.SU, x.PR, x.DP + 2 * S, S, x.M, x.kx, x.ky, 2 * dt * c3, x.s);
   bwd<T>(x, x.U, x.UNL, 3 * x.nz);
   if (stage == 2)
     features<T>((const T*)x.UNL, x.nx, x.ny, x.nz, x.glz, x.lmx, x.lmy, x.bits, x.feat, x.DU, S, x.M, x.s);
@@ -685,15 +700,10 @@ static void scalar_correct(Ctx& x, int stage) {
     ep.s = 1.0;
     gemm(x, x.opD1, x.F6 + 2 * S, S, x.ADVPHI, S, 1, ep);
   } else {
-    EpiParams ep;
-    ep.mode = EPI_GRAD;
-    ep.kx = x.kx;
-    ep.ky = x.ky;
-    ep.X0 = x.PHI;
-    ep.aux0 = x.TMP;
-    ep.aux1 = x.TMP + S;
-    gemm(x, x.opD1, x.PHI, S, x.TMP + 2 * S, S, 1, ep);
-    bwd<T>(x, x.TMP, dup, 3 * x.nz);
+    gemm(x, x.opD1, x.PHI, S, x.TMP + 2 * S, S, 1, EpiParams());   // d(phi)/dz; x and y on load
+    const double2* src[3] = {x.PHI, x.PHI, x.TMP + 2 * S};
+    const int der[3] = {1, 2, 0};
+    bwd_gather<T>(x, src, der, 3, dup);
     adv_products<T>(unl, dup, prd, P, 1, s0, s1, s2, x.s);
     fwd<T>(x, prd, x.ADVPHI, x.nz);
   }
@@ -807,15 +817,9 @@ static void upload_state(Ctx& x, const double* uvw, const double* p, const doubl
     ref_to_slab(x.REF, x.PHI, x.M, x.nz, 1, x.s);
     TG_CUDA(cudaMemsetAsync(x.HPHI, 0, S * sizeof(double2), x.s));
   }
-  // FlatCarrierVariable::Configure: grad p, physical velocity; fresh registers
-  EpiParams ep;
-  ep.mode = EPI_GRAD;
-  ep.kx = x.kx;
-  ep.ky = x.ky;
-  ep.X0 = x.PR;
-  ep.aux0 = x.DP;
-  ep.aux1 = x.DP + S;
-  gemm(x, x.opD1, x.PR, S, x.DP + 2 * S, S, 1, ep);
+  // FlatCarrierVariable::Configure: grad p (its z component; x and y are
+  // formed from p where they are read), physical velocity; fresh registers
+  gemm(x, x.opD1, x.PR, S, x.DP + 2 * S, S, 1, EpiParams());
   TG_CUDA(cudaMemsetAsync(x.H, 0, 3 * S * sizeof(double2), x.s));
   TG_CUDA(cudaMemsetAsync(x.hist, 0, 24 * (size_t)x.M * sizeof(double2), x.s));
   TG_CUDA(cudaMemsetAsync(x.DU, 0, 9 * S * sizeof(double2), x.s));

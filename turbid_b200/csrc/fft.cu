@@ -145,6 +145,20 @@ __device__ cplx<T>* fft_batch(cplx<T>* b0, cplx<T>* b1, int NB, const PlanArgs& 
 // reads contiguous row blocks), [plane][kx][y] for FP64.
 template <typename T> __host__ __device__ constexpr bool bwd_row_major() { return sizeof(T) == 4; }
 
+// Source plane of a gathered backward launch and the derivative to form on load.
+__device__ __forceinline__ const double2* gather_src(const SpecGather& g, int plane, int nz, int M, int& deriv) {
+  const int gp = g.plane0 + plane, f = gp / nz, z = gp - f * nz;
+  deriv = g.deriv[f];
+  return g.src[f] + (size_t)z * M;
+}
+// coefficient m of the loaded plane, differentiated as (0 + i k) * v (the
+// complex product of SpaceStepper::Gradient, src/stepper_space.cc:373-385)
+__device__ __forceinline__ double2 gather_value(const SpecGather& g, int deriv, int m, double2 v) {
+  if (deriv == 0) return v;
+  const double k = deriv == 1 ? g.kx[m] : g.ky[m];
+  return make_double2(0.0 * v.x - k * v.y, 0.0 * v.y + k * v.x);
+}
+
 // ---------------------------------------------------------------------------
 // compile-time Stockham passes for power-of-two lengths: radix-16 passes
 // while 16 divides the remaining length, then one radix-8/4/2 pass; the small
@@ -266,10 +280,10 @@ __global__ void __launch_bounds__(256) fwd_y_kernel(TransformDims d, PlanArgs pl
 }
 
 // backward y pass: spec -> work (zero-filled pruned modes, unscaled)
-template <typename T, int LC>
+template <typename T, int LC, bool GATHER>
 __global__ void __launch_bounds__(256) bwd_y_kernel(TransformDims d, PlanArgs pl, const cplx<T>* __restrict__ tw,
                                                     const double2* __restrict__ spec, cplx<T>* __restrict__ work,
-                                                    int NB) {
+                                                    int NB, SpecGather gat) {
   using C = cplx<T>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* b0 = reinterpret_cast<C*>(smem_raw);
@@ -279,12 +293,14 @@ __global__ void __launch_bounds__(256) bwd_y_kernel(TransformDims d, PlanArgs pl
   const int k0 = blockIdx.x * NB;
   for (int idx = threadIdx.x; idx < NB * L; idx += blockDim.x) b0[idx] = mkc<C>(0, 0);
   __syncthreads();
-  const double2* src = spec + (size_t)plane * d.M;
+  int deriv = 0;
+  const double2* src = GATHER ? gather_src(gat, plane, d.nz, d.M, deriv) : spec + (size_t)plane * d.M;
   for (int idx = threadIdx.x; idx < NB * d.nyc; idx += blockDim.x) {
     const int c = idx / d.nyc, iy = idx - c * d.nyc;
     const int k = k0 + c;
     if (k >= d.nxh) continue;
-    double2 v = src[iy + (size_t)d.nyc * k];
+    const int m = iy + d.nyc * k;
+    double2 v = GATHER ? gather_value(gat, deriv, m, src[m]) : src[m];
     b0[c * L + d.yidx[iy]] = mkc<C>((T)v.x, (T)v.y);
   }
   __syncthreads();
@@ -477,10 +493,10 @@ __global__ void __launch_bounds__(NB * L / 16) fy_p2_kernel(TransformDims d, con
 }
 
 // backward y pass: zero-filled pruned modes, unscaled
-template <typename T, int L, int NB>
+template <typename T, int L, int NB, bool GATHER>
 __global__ void __launch_bounds__(NB * L / 16) by_p2_kernel(TransformDims d, const cplx<T>* __restrict__ tw,
                                                            const double2* __restrict__ spec,
-                                                           cplx<T>* __restrict__ work) {
+                                                           cplx<T>* __restrict__ work, SpecGather gat) {
   using C = cplx<T>;
   constexpr int RS = P2<L>::RS, NT = NB * L / 16;
   constexpr bool RM = P2Vec<T>::kBwdRowMajor;
@@ -494,7 +510,8 @@ __global__ void __launch_bounds__(NB * L / 16) by_p2_kernel(TransformDims d, con
     const int c = idx / gap, y = nyc / 2 + (idx - c * gap);
     buf[c * RS + sp(y)] = mkc<C>(0, 0);
   }
-  const double2* src = spec + (size_t)plane * d.M;
+  int deriv = 0;
+  const double2* src = GATHER ? gather_src(gat, plane, d.nz, d.M, deriv) : spec + (size_t)plane * d.M;
   if constexpr (RM) {
     // the NB columns are one contiguous run of NB*nyc coefficients; every
     // load in flight before the first shared store
@@ -512,7 +529,8 @@ __global__ void __launch_bounds__(NB * L / 16) by_p2_kernel(TransformDims d, con
       const int idx = threadIdx.x + i * NT;
       if (idx < NB * nyc) {
         const int c = idx / nyc, iy = idx - c * nyc;
-        buf[c * RS + sp(y_of(iy, L, nyc))] = mkc<C>((T)v[i].x, (T)v[i].y);
+        const double2 w = GATHER && idx < run ? gather_value(gat, deriv, k0 * nyc + idx, v[i]) : v[i];
+        buf[c * RS + sp(y_of(iy, L, nyc))] = mkc<C>((T)w.x, (T)w.y);
       }
     }
   } else {
@@ -520,7 +538,8 @@ __global__ void __launch_bounds__(NB * L / 16) by_p2_kernel(TransformDims d, con
     for (int idx = threadIdx.x; idx < NB * nyc; idx += NT) {
       const int c = idx / nyc, iy = idx - c * nyc;
       const int k = k0 + c;
-      double2 v = k < d.nxh ? src[iy + (size_t)nyc * k] : make_double2(0.0, 0.0);
+      const int m = iy + nyc * k;
+      double2 v = k < d.nxh ? (GATHER ? gather_value(gat, deriv, m, src[m]) : src[m]) : make_double2(0.0, 0.0);
       buf[c * RS + sp(y_of(iy, L, nyc))] = mkc<C>((T)v.x, (T)v.y);
     }
   }
@@ -683,7 +702,8 @@ template <typename T, int LC>
 static void set_smem_all() {
   set_smem(fwd_x_kernel<T, LC>);
   set_smem(fwd_y_kernel<T, LC>);
-  set_smem(bwd_y_kernel<T, LC>);
+  set_smem(bwd_y_kernel<T, LC, false>);
+  set_smem(bwd_y_kernel<T, LC, true>);
   set_smem(bwd_x_kernel<T, LC>);
 }
 
@@ -779,7 +799,9 @@ void dft_forward(const TransformDims& d, const FftPlan& px, const FftPlan& py, c
 
 template <typename T>
 void dft_backward(const TransformDims& d, const FftPlan& px, const FftPlan& py, const double2* spec, T* phys,
-                  int planes, void* work, cudaStream_t s) {
+                  int planes, void* work, cudaStream_t s, const SpecGather* gather) {
+  SpecGather gat{};
+  if (gather) gat = *gather;
   using C = cplx<T>;
   C* w = reinterpret_cast<C*>(work);
   {
@@ -790,7 +812,10 @@ void dft_backward(const TransformDims& d, const FftPlan& px, const FftPlan& py, 
   {                                                                                       \
     constexpr int NB = P2Elems<T, P2_BY>::value / LL;                                              \
     dim3 grid((d.nxh + NB - 1) / NB, planes);                                             \
-    by_p2_kernel<T, LL, NB><<<grid, NB * LL / 16, p2_smem<T, LL, P2_BY>(), s>>>(d, tw, spec, w); \
+    if (gather)                                                                                  \
+      by_p2_kernel<T, LL, NB, true><<<grid, NB * LL / 16, p2_smem<T, LL, P2_BY>(), s>>>(d, tw, spec, w, gat); \
+    else                                                                                        \
+      by_p2_kernel<T, LL, NB, false><<<grid, NB * LL / 16, p2_smem<T, LL, P2_BY>(), s>>>(d, tw, spec, w, gat); \
   }
       TG_P2_DISPATCH(py.L, TG_CALL)
 #undef TG_CALL
@@ -799,7 +824,10 @@ void dft_backward(const TransformDims& d, const FftPlan& px, const FftPlan& py, 
       size_t sm = 2 * (size_t)nb * py.L * sizeof(C);
       dim3 grid((d.nxh + nb - 1) / nb, planes);
       const PlanArgs pa = plan_args(py);
-      bwd_y_kernel<T, 0><<<grid, 256, sm, s>>>(d, pa, tw, spec, w, nb);
+      if (gather)
+        bwd_y_kernel<T, 0, true><<<grid, 256, sm, s>>>(d, pa, tw, spec, w, nb, gat);
+      else
+        bwd_y_kernel<T, 0, false><<<grid, 256, sm, s>>>(d, pa, tw, spec, w, nb, gat);
     }
     prof_end(s);
     TG_LAUNCH_CHECK("bwd_y_kernel");
@@ -833,9 +861,9 @@ template void dft_forward<double>(const TransformDims&, const FftPlan&, const Ff
 template void dft_forward<float>(const TransformDims&, const FftPlan&, const FftPlan&, const float*, double2*, int,
                                  void*, cudaStream_t);
 template void dft_backward<double>(const TransformDims&, const FftPlan&, const FftPlan&, const double2*, double*, int,
-                                   void*, cudaStream_t);
+                                   void*, cudaStream_t, const SpecGather*);
 template void dft_backward<float>(const TransformDims&, const FftPlan&, const FftPlan&, const double2*, float*, int,
-                                  void*, cudaStream_t);
+                                  void*, cudaStream_t, const SpecGather*);
 
 }  // namespace tg
 

@@ -273,8 +273,17 @@ __device__ __forceinline__ void wall_rows_d1(const double2* __restrict__ f, int 
 // history rows, store the new pressure-gradient wall rows; with an open top
 // also d(dp/dz)/dz at the walls (rows 0, N-1 of D1 applied to dp/dz).
 // Block (32, 8): 32 columns, 8 rows of the z sum.
-__global__ void k_boundary_update(double2* __restrict__ hist, const double2* __restrict__ dp, size_t S, int M, int nz,
-                                  int opentop, const double* __restrict__ kx, const double* __restrict__ ky,
+// grad p rows: x and y components i kx p, i ky p from p, z component dpz
+__device__ __forceinline__ double2 grad_p_row(const double2* __restrict__ p, const double2* __restrict__ dpz,
+                                              const double* __restrict__ kx, const double* __restrict__ ky, int c,
+                                              size_t o, int m) {
+  if (c == 2) return dpz[o];
+  return mul_i(c == 0 ? kx[m] : ky[m], p[o]);
+}
+
+__global__ void k_boundary_update(double2* __restrict__ hist, const double2* __restrict__ p,
+                                  const double2* __restrict__ dpz, int M, int nz, int opentop,
+                                  const double* __restrict__ kx, const double* __restrict__ ky,
                                   const double* __restrict__ d1r0, const double* __restrict__ d1rn) {
   const size_t R = (size_t)3 * M;
   const int m = blockIdx.x * 32 + threadIdx.x;
@@ -285,11 +294,11 @@ __global__ void k_boundary_update(double2* __restrict__ hist, const double2* __r
     hist[3 * R + i] = hist[1 * R + i];
     hist[6 * R + i] = hist[4 * R + i];
     hist[7 * R + i] = hist[5 * R + i];
-    hist[1 * R + i] = dp[(size_t)c * S + m];
-    hist[0 * R + i] = dp[(size_t)c * S + (size_t)(nz - 1) * M + m];
+    hist[1 * R + i] = grad_p_row(p, dpz, kx, ky, c, (size_t)m, m);
+    hist[0 * R + i] = grad_p_row(p, dpz, kx, ky, c, (size_t)(nz - 1) * M + m, m);
   }
   if (opentop) {
-    const double2* g = dp + 2 * S;  // dp/dz
+    const double2* g = dpz;  // dp/dz
     double2 r0, rn;
     wall_rows_d1(g, M, nz, m, d1r0, d1rn, r0, rn);
     if (threadIdx.y == 0 && m < M) {
@@ -303,10 +312,10 @@ __global__ void k_boundary_update(double2* __restrict__ hist, const double2* __r
     }
   }
 }
-void boundary_update(double2* hist, const double2* dp, size_t S, int M, int nz, int opentop, const double* kx,
-                     const double* ky, const double* d1r0, const double* d1rn, cudaStream_t s) {
+void boundary_update(double2* hist, const double2* p, const double2* dpz, int M, int nz, int opentop,
+                     const double* kx, const double* ky, const double* d1r0, const double* d1rn, cudaStream_t s) {
   prof_begin(s, PC_ELEM, 16.0 * (double)M * (opentop ? nz + 16 : 16), 0);
-  k_boundary_update<<<(M + 31) / 32, dim3(32, 8), 0, s>>>(hist, dp, S, M, nz, opentop, kx, ky, d1r0, d1rn);
+  k_boundary_update<<<(M + 31) / 32, dim3(32, 8), 0, s>>>(hist, p, dpz, M, nz, opentop, kx, ky, d1r0, d1rn);
   prof_end(s);
   TG_LAUNCH_CHECK("k_boundary_update");
 }
@@ -336,21 +345,24 @@ void wall_dz(const double2* U, double2* DU, size_t S, int M, int nz, const doubl
 }
 
 // projection u = u* - 2 dt c3 grad p, mean w := 0 (phase_carrier_flat.cc:609-620)
-__global__ void k_project(double2* __restrict__ U, const double2* __restrict__ SU, const double2* __restrict__ DP,
-                          size_t S, int M, double coef) {
+__global__ void k_project(double2* __restrict__ U, const double2* __restrict__ SU, const double2* __restrict__ P,
+                          const double2* __restrict__ DPZ, size_t S, int M, const double* __restrict__ kx,
+                          const double* __restrict__ ky, double coef) {
   const size_t n = 3 * S;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
     const int c = (int)(i / S);
     const size_t e = i - (size_t)c * S;
-    double2 su = SU[i], dp = DP[i];
+    const int m = (int)(e % M);
+    double2 su = SU[i], dp = grad_p_row(P, DPZ, kx, ky, c, e, m);
     double2 u = make_double2(su.x - coef * dp.x, su.y - coef * dp.y);
-    if (c == 2 && (e % M) == 0) u = make_double2(0.0, 0.0);
+    if (c == 2 && m == 0) u = make_double2(0.0, 0.0);
     U[i] = u;
   }
 }
-void project(double2* U, const double2* SU, const double2* DP, size_t S, int M, double coef, cudaStream_t s) {
-  prof_begin(s, PC_ELEM, 144.0 * (double)S, 0);
-  k_project<<<nblk(3 * S), kT, 0, s>>>(U, SU, DP, S, M, coef);
+void project(double2* U, const double2* SU, const double2* P, const double2* DPZ, size_t S, int M, const double* kx,
+             const double* ky, double coef, cudaStream_t s) {
+  prof_begin(s, PC_ELEM, 112.0 * (double)S, 0);   // SU (3), p, dp/dz in; U (3) out
+  k_project<<<nblk(3 * S), kT, 0, s>>>(U, SU, P, DPZ, S, M, kx, ky, coef);
   prof_end(s);
   TG_LAUNCH_CHECK("k_project");
 }

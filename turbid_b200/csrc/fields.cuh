@@ -22,11 +22,13 @@ void h_update(double2* H, const double2* adv, const double2* phi, size_t S, int 
 void axmby(double2* y, const double2* x, size_t n, double a, double b, cudaStream_t s);
 void boundary_apply(double2* rhs, const double2* hist, size_t S, int M, int nz, double fac, double r, int opentop,
                     double tu, double tv, double tw, cudaStream_t s);
-void boundary_update(double2* hist, const double2* dp, size_t S, int M, int nz, int opentop, const double* kx,
-                     const double* ky, const double* d1r0, const double* d1rn, cudaStream_t s);
+// grad p enters as p (x and y components i kx p, i ky p) and dp/dz
+void boundary_update(double2* hist, const double2* p, const double2* dpz, int M, int nz, int opentop,
+                     const double* kx, const double* ky, const double* d1r0, const double* d1rn, cudaStream_t s);
 void wall_dz(const double2* U, double2* DU, size_t S, int M, int nz, const double* d1r0, const double* d1rn,
              cudaStream_t s);
-void project(double2* U, const double2* SU, const double2* DP, size_t S, int M, double coef, cudaStream_t s);
+void project(double2* U, const double2* SU, const double2* P, const double2* DPZ, size_t S, int M, const double* kx,
+             const double* ky, double coef, cudaStream_t s);
 void zero_rows(double2* f, int M, int nz, cudaStream_t s);
 template <typename T>
 void erosion_tau(const T* dudz, const T* dvdz, T* tau, size_t n, double re, double tauc, double rate,

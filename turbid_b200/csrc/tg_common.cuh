@@ -107,9 +107,23 @@ struct TransformDims {
 template <typename T>
 void dft_forward(const TransformDims& d, const FftPlan& px, const FftPlan& py,
                  const T* phys, double2* spec, int planes, void* work, cudaStream_t s);
+// Sources of a backward transform launch, one per field of nz planes: the
+// spectral field as it is (deriv 0) or its x (1: i kx) or y (2: i ky)
+// derivative, formed as the coefficients are loaded.  plane0 is the global
+// plane index of the launch's first plane.
+constexpr int kMaxGather = 9;
+struct SpecGather {
+  const double2* src[kMaxGather];
+  int deriv[kMaxGather];
+  const double* kx;
+  const double* ky;
+  int nf;       // fields; 0: plain contiguous source
+  int plane0;
+};
 template <typename T>
 void dft_backward(const TransformDims& d, const FftPlan& px, const FftPlan& py,
-                  const double2* spec, T* phys, int planes, void* work, cudaStream_t s);
+                  const double2* spec, T* phys, int planes, void* work, cudaStream_t s,
+                  const SpecGather* gather = nullptr);
 
 // ---------------------------------------------------------------------------
 // z-operator GEMM (gemm.cu):  out[r][m] = epi( sum_k A[r][k] in[k][m] )
