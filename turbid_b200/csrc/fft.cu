@@ -519,17 +519,25 @@ __global__ void __launch_bounds__(NB * L / 16) by_p2_kernel(TransformDims d, con
     const int run = min(NB, d.nxh - k0) * nyc;
     const double2* s0 = src + (size_t)k0 * nyc;
     double2 v[IT];
+    double kf[GATHER ? IT : 1];   // wavenumber of a derivative, loaded with the coefficient
 #pragma unroll
     for (int i = 0; i < IT; ++i) {
       const int idx = threadIdx.x + i * NT;
       v[i] = idx < run ? s0[idx] : make_double2(0.0, 0.0);
+      if constexpr (GATHER) {
+        const double* kt = deriv == 1 ? gat.kx : gat.ky;
+        kf[i] = (deriv != 0 && idx < run) ? kt[k0 * nyc + idx] : 0.0;
+      }
     }
 #pragma unroll
     for (int i = 0; i < IT; ++i) {
       const int idx = threadIdx.x + i * NT;
       if (idx < NB * nyc) {
         const int c = idx / nyc, iy = idx - c * nyc;
-        const double2 w = GATHER && idx < run ? gather_value(gat, deriv, k0 * nyc + idx, v[i]) : v[i];
+        double2 w = v[i];
+        if constexpr (GATHER) {
+          if (deriv != 0) w = make_double2(0.0 * v[i].x - kf[i] * v[i].y, 0.0 * v[i].y + kf[i] * v[i].x);
+        }
         buf[c * RS + sp(y_of(iy, L, nyc))] = mkc<C>((T)w.x, (T)w.y);
       }
     }
