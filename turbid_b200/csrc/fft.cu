@@ -482,7 +482,7 @@ __global__ void __launch_bounds__(NB * L / 16) fy_p2_kernel(TransformDims d, con
   __syncthreads();
   ip_passes<T, -1, L, NB, 1>(buf, tw);
   double2* dst = spec + (size_t)plane * d.M;
-  const int nyc = d.nyc;
+  constexpr int nyc = L / 3 * 2;   // d.nyc of a power-of-two Ny = L
   for (int idx = threadIdx.x; idx < NB * nyc; idx += NT) {
     const int c = idx / nyc, iy = idx - c * nyc;
     const int k = k0 + c;
@@ -504,8 +504,8 @@ __global__ void __launch_bounds__(NB * L / 16) by_p2_kernel(TransformDims d, con
   C* buf = reinterpret_cast<C*>(smem_raw);
   const int plane = blockIdx.y;
   const int k0 = blockIdx.x * NB;
-  const int nyc = d.nyc;
-  const int gap = L - nyc;  // FFT indices [nyc/2, L - nyc/2) carry no spectral row
+  constexpr int nyc = L / 3 * 2;   // d.nyc of a power-of-two Ny = L
+  constexpr int gap = L - nyc;  // FFT indices [nyc/2, L - nyc/2) carry no spectral row
   for (int idx = threadIdx.x; idx < NB * gap; idx += NT) {
     const int c = idx / gap, y = nyc / 2 + (idx - c * gap);
     buf[c * RS + sp(y)] = mkc<C>(0, 0);
@@ -583,8 +583,8 @@ __global__ void __launch_bounds__(NB * L / 16) bx_p2_kernel(TransformDims d, con
   C* buf = reinterpret_cast<C*>(smem_raw);
   const int plane = blockIdx.y;
   const int y0 = blockIdx.x * rows;
-  const int nxh = d.nxh;
-  const int gap = L - 2 * nxh + 1;  // FFT indices [nxh, L - nxh] are zero
+  constexpr int nxh = L / 3 * 2 / 2 + 1;   // d.nxh of a power-of-two Nx = L
+  constexpr int gap = L - 2 * nxh + 1;  // FFT indices [nxh, L - nxh] are zero
   for (int idx = threadIdx.x; idx < NB * gap; idx += NT) {
     const int p = idx / gap, x = nxh + (idx - p * gap);
     buf[p * RS + sp(x)] = mkc<C>(0, 0);
@@ -761,7 +761,7 @@ void dft_forward(const TransformDims& d, const FftPlan& px, const FftPlan& py, c
   {
     prof_begin(s, PC_FFT_FX, (double)planes * d.ny * (d.nx * sizeof(T) + d.nxh * sizeof(C)), 0);
     const C* tw = Tw<T>::get(px);
-    if (p2_length(px.L) && aligned16(phys)) {
+    if (p2_length(px.L) && aligned16(phys) && d.nxh == px.L / 3 * 2 / 2 + 1) {
 #define TG_CALL(LL)                                                                         \
   {                                                                                         \
     constexpr int NB = P2Elems<T, P2_FX>::value / LL;                                                \
@@ -784,7 +784,7 @@ void dft_forward(const TransformDims& d, const FftPlan& px, const FftPlan& py, c
     const double scale = 1.0 / ((double)d.nx * (double)d.ny);
     prof_begin(s, PC_FFT_FY, (double)planes * ((double)d.nxh * d.ny * sizeof(C) + (double)d.M * sizeof(double2)), 0);
     const C* tw = Tw<T>::get(py);
-    if (p2_length(py.L)) {
+    if (p2_length(py.L) && d.nyc == py.L / 3 * 2) {
 #define TG_CALL(LL)                                                                              \
   {                                                                                              \
     constexpr int NB = P2Elems<T, P2_FY>::value / LL;                                                     \
@@ -815,7 +815,7 @@ void dft_backward(const TransformDims& d, const FftPlan& px, const FftPlan& py, 
   {
     prof_begin(s, PC_FFT_BY, (double)planes * ((double)d.nxh * d.ny * sizeof(C) + (double)d.M * sizeof(double2)), 0);
     const C* tw = Tw<T>::get(py);
-    if (p2_length(py.L)) {
+    if (p2_length(py.L) && d.nyc == py.L / 3 * 2) {
 #define TG_CALL(LL)                                                                       \
   {                                                                                       \
     constexpr int NB = P2Elems<T, P2_BY>::value / LL;                                              \
@@ -843,7 +843,7 @@ void dft_backward(const TransformDims& d, const FftPlan& px, const FftPlan& py, 
   {
     prof_begin(s, PC_FFT_BX, (double)planes * d.ny * (d.nx * sizeof(T) + d.nxh * sizeof(C)), 0);
     const C* tw = Tw<T>::get(px);
-    if (p2_length(px.L) && aligned16(phys)) {
+    if (p2_length(px.L) && aligned16(phys) && d.nxh == px.L / 3 * 2 / 2 + 1) {
 #define TG_CALL(LL)                                                                       \
   {                                                                                       \
     constexpr int NB = P2Elems<T, P2_BX>::value / LL;                                              \
