@@ -548,12 +548,12 @@ static void carrier_predict(Ctx& x, int stage) {
   }
   double f1, f2;
   mean_force(x, f1, f2);
-  if (x.sc_pending) {  // phi of the previous stage's scalar Correct (second stream)
-    TG_CUDA(cudaStreamWaitEvent(x.s, x.sc_done, 0));
-    x.sc_pending = false;
-  }
-  h_update(x.H, x.ADV, phi, S, x.M, c1, dt, bcoef, std::sin(x.c.slope), std::cos(x.c.slope), x.c.slope_direction,
-           dt * f1, dt * f2, x.capturing ? x.force_d : nullptr, x.s);
+  // The buoyancy term needs phi from the previous stage's scalar Correct
+  // (possibly still running on the second stream): it is added after the
+  // right-hand side, just before the solves of the components it enters, so
+  // that the H update, the Laplacian and the u/v solves do not wait for it.
+  h_update(x.H, x.ADV, nullptr, S, x.M, c1, dt, 0.0, 0.0, 0.0, 0, dt * f1, dt * f2,
+           x.capturing ? x.force_d : nullptr, x.s);
   // Laplacian and rhs (phase_carrier_flat.cc:517-536)
   {
     const double redtc3 = -x.c.reynolds / dt / c3;
@@ -608,16 +608,39 @@ static void carrier_predict(Ctx& x, int stage) {
       fwd[i] = ZProblem{&x.opEinv[i], x.RHS + i * S, (long long)S, x.TMP + i * S, (long long)S, 1, ep};
       bwd[i] = ZProblem{&x.opE[i], x.TMP + i * S, (long long)S, x.SU + i * S, (long long)S, 1, EpiParams()};
     }
+    // buoyancy: w always (-cos of the slope), u or v along a sloped bed (+sin)
+    const int sdir = x.c.slope_direction;
+    const double ac2 = (-x.c.reynolds / dt / c3) * c2;   // coefficient of H in the rhs
+    auto add_buoyancy = [&](int c, cudaStream_t st) {
+      if (!phi) return;
+      if (c == 2)
+        buoyancy(x.H + 2 * S, x.RHS + 2 * S, phi, x.M, x.nz, bcoef, std::cos(x.c.slope), -1, ac2, st);
+      else if ((sdir == 1 && c == 0) || (sdir == 2 && c == 1))
+        buoyancy(x.H + c * S, x.RHS + c * S, phi, x.M, x.nz, bcoef, std::sin(x.c.slope), +1, ac2, st);
+    };
     if (x.fork_active && x.opEinv[2].sym && x.opE[2].sym) {
       TG_CUDA(cudaEventRecord(x.w_fork, x.s));
       TG_CUDA(cudaStreamWaitEvent(x.s3, x.w_fork, 0));
+      if (x.sc_pending) TG_CUDA(cudaStreamWaitEvent(x.s3, x.sc_done, 0));
+      add_buoyancy(2, x.s3);
       zgemm_group(&fwd[2], 1, x.M, x.s3);
       zgemm_group(&bwd[2], 1, x.M, x.s3);
       TG_CUDA(cudaEventRecord(x.w_join, x.s3));
+      if (phi && sdir != 0) {  // a sloped bed: u or v waits for phi too
+        if (x.sc_pending) TG_CUDA(cudaStreamWaitEvent(x.s, x.sc_done, 0));
+        add_buoyancy(0, x.s);
+        add_buoyancy(1, x.s);
+      }
       zgemm_group(fwd, 2, x.M, x.s);
       zgemm_group(bwd, 2, x.M, x.s);
-      TG_CUDA(cudaStreamWaitEvent(x.s, x.w_join, 0));
+      TG_CUDA(cudaStreamWaitEvent(x.s, x.w_join, 0));   // also after the scalar Correct
+      x.sc_pending = false;
     } else {
+      if (x.sc_pending) {
+        TG_CUDA(cudaStreamWaitEvent(x.s, x.sc_done, 0));
+        x.sc_pending = false;
+      }
+      for (int c = 0; c < 3; ++c) add_buoyancy(c, x.s);
       zgemm_group(fwd, 3, x.M, x.s);
       zgemm_group(bwd, 3, x.M, x.s);
     }

@@ -185,6 +185,49 @@ void h_update(double2* H, const double2* adv, const double2* phi, size_t S, int 
   TG_LAUNCH_CHECK("k_h_update");
 }
 
+// Buoyancy of the H update (phase_carrier_flat.cc:325-356), added after the
+// right-hand side has been formed: component H_c gets sgn * bcoef * phi * trig
+// (the H update's own expression), and the interior rows of the right-hand
+// side the same term times a*c2, its coefficient of H in the Laplacian/rhs
+// step (rows 0 and N-1 already hold the boundary values).  This lets the
+// carrier's H update, Laplacian and u/v solves run before the scalar Correct
+// that produces phi has finished.
+__global__ void k_buoyancy(double2* __restrict__ H, double2* __restrict__ rhs, const double2* __restrict__ phi, int M,
+                           int nz, double bcoef, double trig, int sgn, double ac2) {
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= M) return;
+  const int z = blockIdx.y;
+  const size_t e = (size_t)z * M + m;
+  const double2 p = phi[e];
+  double2 h = H[e];
+  double tx, ty;
+  if (sgn > 0) {
+    h.x = h.x + bcoef * p.x * trig;
+    h.y = h.y + bcoef * p.y * trig;
+    tx = bcoef * p.x * trig;
+    ty = bcoef * p.y * trig;
+  } else {
+    h.x = h.x - bcoef * p.x * trig;
+    h.y = h.y - bcoef * p.y * trig;
+    tx = -(bcoef * p.x * trig);
+    ty = -(bcoef * p.y * trig);
+  }
+  H[e] = h;
+  if (z != 0 && z != nz - 1) {
+    double2 r = rhs[e];
+    r.x += ac2 * tx;
+    r.y += ac2 * ty;
+    rhs[e] = r;
+  }
+}
+void buoyancy(double2* H, double2* rhs, const double2* phi, int M, int nz, double bcoef, double trig, int sgn,
+              double ac2, cudaStream_t s) {
+  prof_begin(s, PC_ELEM, 80.0 * (double)M * nz, 0);
+  k_buoyancy<<<dim3((M + kT - 1) / kT, nz), kT, 0, s>>>(H, rhs, phi, M, nz, bcoef, trig, sgn, ac2);
+  prof_end(s);
+  TG_LAUNCH_CHECK("k_buoyancy");
+}
+
 // scalar register (phase_scalar_flat.cc:308-310)
 __global__ void k_axpby(double2* __restrict__ y, const double2* __restrict__ x, size_t n, double a, double b) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {

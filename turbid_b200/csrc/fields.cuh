@@ -19,6 +19,9 @@ template <typename T> void mul_shift(const T* a, const T* b, T* out, size_t P, d
 void h_update(double2* H, const double2* adv, const double2* phi, size_t S, int M, double c1, double dt,
               double bcoef, double sinsl, double cossl, int sdir, double dtf1, double dtf2, const double* dtf,
               cudaStream_t s);
+// H_c += sgn * bcoef * phi * trig; interior rows of rhs_c += a*c2 times that term
+void buoyancy(double2* H, double2* rhs, const double2* phi, int M, int nz, double bcoef, double trig, int sgn,
+              double ac2, cudaStream_t s);
 void axmby(double2* y, const double2* x, size_t n, double a, double b, cudaStream_t s);
 void boundary_apply(double2* rhs, const double2* hist, size_t S, int M, int nz, double fac, double r, int opentop,
                     double tu, double tv, double tw, cudaStream_t s);
