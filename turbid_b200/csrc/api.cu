@@ -421,6 +421,16 @@ static void bwd(Ctx& x, const double2* spec, void* phys, int planes) {
   }
 }
 
+// Forward transform of nf products a[f] * (b[f] + sh[f]) of physical fields,
+// formed as the x pass loads its rows (one launch pair); false when the grid or
+// the scratch does not allow it (the caller then forms the products itself).
+template <typename T>
+static bool fwd_products(Ctx& x, const PhysProduct& pp, double2* spec) {
+  if (pp.nf * x.nz > x.work_planes || !dft_forward_products_ok<T>(x.td, x.px, pp)) return false;
+  dft_forward<T>(x.td, x.px, x.py, nullptr, spec, pp.nf * x.nz, x.work, x.s, &pp);
+  return true;
+}
+
 // Backward transforms of nf fields gathered from their own spectral sources,
 // the x and y derivatives (deriv 1, 2) formed as the coefficients are loaded:
 // the spectral derivative fields are never written.
@@ -500,8 +510,20 @@ static void carrier_predict(Ctx& x, int stage) {
   };
   // NonlinearVelocity (phase_carrier_flat.cc:716-813)
   if (x.alternation) {
-    products6<T>(unl, prd, P, x.s);
-    fwd<T>(x, prd, x.F6, 6 * x.nz);
+    {  // the six products u_i u_j, formed as the forward transform loads its rows
+      PhysProduct pp{};
+      const int ia[6] = {0, 0, 0, 1, 1, 2}, ib[6] = {0, 1, 2, 1, 2, 2};
+      for (int f = 0; f < 6; ++f) {
+        pp.a[f] = unl + ia[f] * P;
+        pp.b[f] = unl + ib[f] * P;
+        pp.sh[f] = 0.0;
+      }
+      pp.nf = 6;
+      if (!fwd_products<T>(x, pp, x.F6)) {
+        products6<T>(unl, prd, P, x.s);
+        fwd<T>(x, prd, x.F6, 6 * x.nz);
+      }
+    }
     // adv_i = d/dx(u_i u) + d/dy(u_i v) + d/dz(u_i w): GradientTmp + sum
     const int inI[3] = {2, 4, 5}, x0I[3] = {0, 1, 2}, x1I[3] = {1, 3, 4};
     ZProblem pr[3];
@@ -712,8 +734,18 @@ static void scalar_correct(Ctx& x, int stage) {
   // NonlinearPressure (phase_scalar_flat.cc:552-599)
   if (x.alternation) {
     bwd<T>(x, x.PHI, phip, x.nz);
-    phi_products<T>(phip, unl, prd, P, s0, s1, s2, x.s);
-    fwd<T>(x, prd, x.F6, 3 * x.nz);
+    PhysProduct pp{};  // phi (u_j + shift_j), formed as the forward transform loads its rows
+    const double shj[3] = {s0, s1, s2};
+    for (int f = 0; f < 3; ++f) {
+      pp.a[f] = phip;
+      pp.b[f] = unl + f * P;
+      pp.sh[f] = shj[f];
+    }
+    pp.nf = 3;
+    if (!fwd_products<T>(x, pp, x.F6)) {
+      phi_products<T>(phip, unl, prd, P, s0, s1, s2, x.s);
+      fwd<T>(x, prd, x.F6, 3 * x.nz);
+    }
     EpiParams ep;
     ep.mode = EPI_DIV;
     ep.kx = x.kx;

@@ -396,21 +396,34 @@ __device__ __forceinline__ void cset(double2& v, int, double2 a) { v = a; }
 template <typename V> __device__ __forceinline__ V vzero() { V v; memset(&v, 0, sizeof(V)); return v; }
 
 // forward x pass, L = nx: NB row pairs per CTA, 2 rows packed per complex FFT
-template <typename T, int L, int NB>
+template <typename T, int L, int NB, bool PROD>
 __global__ void __launch_bounds__(NB * L / 16) fx_p2_kernel(TransformDims d, const cplx<T>* __restrict__ tw,
-                                                           const T* __restrict__ phys, cplx<T>* __restrict__ work) {
+                                                           const T* __restrict__ phys, cplx<T>* __restrict__ work,
+                                                           PhysProduct prod) {
   using C = cplx<T>;
   using PV = P2Vec<T>;
   using R = typename PV::R;
   constexpr int VW = PV::VW, RS = P2<L>::RS, NT = NB * L / 16, rows = 2 * NB;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* buf = reinterpret_cast<C*>(smem_raw);
-  const int plane = blockIdx.y;
+  int plane = blockIdx.y;
   const int y0 = blockIdx.x * rows;
-  const T* src = phys + (size_t)plane * d.ny * L;
+  const T* src;
+  const T* srcb = nullptr;
+  T shb = T(0);
+  if constexpr (PROD) {  // planes z-major: z = blockIdx.y / nf, field f; output plane f*nz + z
+    const int z = plane / prod.nf, f = plane - z * prod.nf;
+    src = reinterpret_cast<const T*>(prod.a[f]) + (size_t)z * d.ny * L;
+    if (prod.b[f]) srcb = reinterpret_cast<const T*>(prod.b[f]) + (size_t)z * d.ny * L;
+    shb = (T)prod.sh[f];
+    plane = f * d.nz + z;
+  } else {
+    src = phys + (size_t)plane * d.ny * L;
+  }
   {
     constexpr int IT = NB * L / (NT * VW);  // every load of the tile in flight before the first shared store
     R va[IT], vb[IT];
+    R wa[PROD ? IT : 1], wb[PROD ? IT : 1];
 #pragma unroll
     for (int i = 0; i < IT; ++i) {
       const int e = (threadIdx.x + i * NT) * VW;
@@ -418,6 +431,23 @@ __global__ void __launch_bounds__(NB * L / 16) fx_p2_kernel(TransformDims d, con
       const int ya = y0 + 2 * p, yb = ya + 1;
       va[i] = ya < d.ny ? *reinterpret_cast<const R*>(src + (size_t)ya * L + x) : vzero<R>();
       vb[i] = yb < d.ny ? *reinterpret_cast<const R*>(src + (size_t)yb * L + x) : vzero<R>();
+      if constexpr (PROD) {
+        if (srcb) {
+          wa[i] = ya < d.ny ? *reinterpret_cast<const R*>(srcb + (size_t)ya * L + x) : vzero<R>();
+          wb[i] = yb < d.ny ? *reinterpret_cast<const R*>(srcb + (size_t)yb * L + x) : vzero<R>();
+        }
+      }
+    }
+    if constexpr (PROD) {
+      if (srcb) {  // a * (b + shift), the products of the reference's physical-space step
+#pragma unroll
+        for (int i = 0; i < IT; ++i)
+#pragma unroll
+          for (int j = 0; j < VW; ++j) {
+            vset(va[i], j, vget(va[i], j) * (vget(wa[i], j) + shb));
+            vset(vb[i], j, vget(vb[i], j) * (vget(wb[i], j) + shb));
+          }
+      }
     }
 #pragma unroll
     for (int i = 0; i < IT; ++i) {
@@ -754,19 +784,36 @@ static size_t p2_smem() {
 }
 
 template <typename T>
+bool dft_forward_products_ok(const TransformDims& d, const FftPlan& px, const PhysProduct& prod) {
+  if (!p2_length(px.L) || d.nxh != px.L / 3 * 2 / 2 + 1 || prod.nf < 1 || prod.nf > kMaxGather) return false;
+  for (int f = 0; f < prod.nf; ++f)
+    if (!prod.a[f] || !aligned16(prod.a[f]) || (prod.b[f] && !aligned16(prod.b[f]))) return false;
+  return true;
+}
+
+template <typename T>
 void dft_forward(const TransformDims& d, const FftPlan& px, const FftPlan& py, const T* phys, double2* spec,
-                 int planes, void* work, cudaStream_t s) {
+                 int planes, void* work, cudaStream_t s, const PhysProduct* prod) {
   using C = cplx<T>;
   C* w = reinterpret_cast<C*>(work);
+  PhysProduct pp{};
+  if (prod) {
+    if (!dft_forward_products_ok<T>(d, px, *prod) || planes != prod->nf * d.nz)
+      throw Error{TG_ERR_SHAPE, "RealCplxCube::DftForward > products on load need a power-of-two Nx"};
+    pp = *prod;
+  }
   {
     prof_begin(s, PC_FFT_FX, (double)planes * d.ny * (d.nx * sizeof(T) + d.nxh * sizeof(C)), 0);
     const C* tw = Tw<T>::get(px);
-    if (p2_length(px.L) && aligned16(phys) && d.nxh == px.L / 3 * 2 / 2 + 1) {
+    if (prod || (p2_length(px.L) && aligned16(phys) && d.nxh == px.L / 3 * 2 / 2 + 1)) {
 #define TG_CALL(LL)                                                                         \
   {                                                                                         \
     constexpr int NB = P2Elems<T, P2_FX>::value / LL;                                                \
     dim3 grid((d.ny + 2 * NB - 1) / (2 * NB), planes);                                      \
-    fx_p2_kernel<T, LL, NB><<<grid, NB * LL / 16, p2_smem<T, LL, P2_FX>(), s>>>(d, tw, phys, w);   \
+    if (prod)                                                                               \
+      fx_p2_kernel<T, LL, NB, true><<<grid, NB * LL / 16, p2_smem<T, LL, P2_FX>(), s>>>(d, tw, phys, w, pp); \
+    else                                                                                    \
+      fx_p2_kernel<T, LL, NB, false><<<grid, NB * LL / 16, p2_smem<T, LL, P2_FX>(), s>>>(d, tw, phys, w, pp); \
   }
       TG_P2_DISPATCH(px.L, TG_CALL)
 #undef TG_CALL
@@ -865,9 +912,11 @@ void dft_backward(const TransformDims& d, const FftPlan& px, const FftPlan& py, 
 }
 
 template void dft_forward<double>(const TransformDims&, const FftPlan&, const FftPlan&, const double*, double2*, int,
-                                  void*, cudaStream_t);
+                                  void*, cudaStream_t, const PhysProduct*);
 template void dft_forward<float>(const TransformDims&, const FftPlan&, const FftPlan&, const float*, double2*, int,
-                                 void*, cudaStream_t);
+                                 void*, cudaStream_t, const PhysProduct*);
+template bool dft_forward_products_ok<double>(const TransformDims&, const FftPlan&, const PhysProduct&);
+template bool dft_forward_products_ok<float>(const TransformDims&, const FftPlan&, const PhysProduct&);
 template void dft_backward<double>(const TransformDims&, const FftPlan&, const FftPlan&, const double2*, double*, int,
                                    void*, cudaStream_t, const SpecGather*);
 template void dft_backward<float>(const TransformDims&, const FftPlan&, const FftPlan&, const double2*, float*, int,

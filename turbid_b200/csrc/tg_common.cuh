@@ -104,14 +104,29 @@ struct TransformDims {
 
 // Transforms (fft.cu).  planes = dim * nz; work = Nxh*Ny complex per plane
 // of the transform precision.
+constexpr int kMaxGather = 9;
+
+// Physical fields of a forward transform launch formed as products on load:
+// field f = a[f] * (b[f] + sh[f]) (b[f] null: a[f] as it is), each factor a
+// physical field of nz planes.  The launch walks the planes z-major, so the
+// factors of one z plane are read from HBM once and then from L2.
+struct PhysProduct {
+  const void* a[kMaxGather];
+  const void* b[kMaxGather];
+  double sh[kMaxGather];
+  int nf;
+};
 template <typename T>
 void dft_forward(const TransformDims& d, const FftPlan& px, const FftPlan& py,
-                 const T* phys, double2* spec, int planes, void* work, cudaStream_t s);
+                 const T* phys, double2* spec, int planes, void* work, cudaStream_t s,
+                 const PhysProduct* prod = nullptr);
+// whether dft_forward can form these products on load (power-of-two Nx, 16-byte aligned factors)
+template <typename T>
+bool dft_forward_products_ok(const TransformDims& d, const FftPlan& px, const PhysProduct& prod);
 // Sources of a backward transform launch, one per field of nz planes: the
 // spectral field as it is (deriv 0) or its x (1: i kx) or y (2: i ky)
 // derivative, formed as the coefficients are loaded.  plane0 is the global
 // plane index of the launch's first plane.
-constexpr int kMaxGather = 9;
 struct SpecGather {
   const double2* src[kMaxGather];
   int deriv[kMaxGather];
