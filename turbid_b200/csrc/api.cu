@@ -421,6 +421,28 @@ static void bwd(Ctx& x, const double2* spec, void* phys, int planes) {
   }
 }
 
+// Backward transforms of ncomp groups of three gradient fields (spectral
+// sources, x/y derivatives formed on load) reduced on the x pass to the
+// advection terms (u+su) d/dx + (v+sv) d/dy + (w+sw) d/dz of each group; false
+// when the grid or the scratch does not allow it.
+template <typename T>
+static bool bwd_advection(Ctx& x, const double2* const* src, const int* deriv, int ncomp, const T* unl, T* out,
+                          double su, double sv, double sw) {
+  const int nf = 3 * ncomp;
+  if (nf * x.nz > x.work_planes || !dft_backward_adv_ok<T>(x.td, x.px, x.py, unl, out)) return false;
+  SpecGather g{};
+  for (int f = 0; f < nf; ++f) {
+    g.src[f] = src[f];
+    g.deriv[f] = deriv[f];
+  }
+  g.kx = x.kx;
+  g.ky = x.ky;
+  g.nf = nf;
+  g.plane0 = 0;
+  dft_backward_adv<T>(x.td, x.px, x.py, g, ncomp, unl, out, su, sv, sw, x.work, x.s);
+  return true;
+}
+
 // Forward transform of nf products a[f] * (b[f] + sh[f]) of physical fields,
 // formed as the x pass loads its rows (one launch pair); false when the grid or
 // the scratch does not allow it (the caller then forms the products itself).
@@ -551,8 +573,10 @@ static void carrier_predict(Ctx& x, int stage) {
       src[3 * i + 2] = x.DU + (3 * i + 2) * S;
       der[3 * i + 2] = 0;
     }
-    bwd_gather<T>(x, src, der, 9, dup);
-    adv_products<T>(unl, dup, prd, P, 3, 0.0, 0.0, 0.0, x.s);
+    if (!bwd_advection<T>(x, src, der, 3, unl, prd, 0.0, 0.0, 0.0)) {
+      bwd_gather<T>(x, src, der, 9, dup);
+      adv_products<T>(unl, dup, prd, P, 3, 0.0, 0.0, 0.0, x.s);
+    }
     fwd<T>(x, prd, x.ADV, 3 * x.nz);
   }
   if (x.scalar && x.c.scalar_bc == 1) {
@@ -758,8 +782,10 @@ static void scalar_correct(Ctx& x, int stage) {
     gemm(x, x.opD1, x.PHI, S, x.TMP + 2 * S, S, 1, EpiParams());   // d(phi)/dz; x and y on load
     const double2* src[3] = {x.PHI, x.PHI, x.TMP + 2 * S};
     const int der[3] = {1, 2, 0};
-    bwd_gather<T>(x, src, der, 3, dup);
-    adv_products<T>(unl, dup, prd, P, 1, s0, s1, s2, x.s);
+    if (!bwd_advection<T>(x, src, der, 1, unl, prd, s0, s1, s2)) {
+      bwd_gather<T>(x, src, der, 3, dup);
+      adv_products<T>(unl, dup, prd, P, 1, s0, s1, s2, x.s);
+    }
     fwd<T>(x, prd, x.ADVPHI, x.nz);
   }
   axmby(x.HPHI, x.ADVPHI, S, c1, dt, x.s);

@@ -602,17 +602,14 @@ __global__ void __launch_bounds__(NB * L / 16) by_p2_kernel(TransformDims d, con
 }
 
 // backward x pass, L = nx: two rows per complex FFT; Im of the kx = 0 coefficient ignored (c2r).
+// Backward x pass, loading half: the zero gap and the row pairs of one work
+// plane combined into the packed two-row FFT input in buf (shared memory).
 template <typename T, int L, int NB>
-__global__ void __launch_bounds__(NB * L / 16) bx_p2_kernel(TransformDims d, const cplx<T>* __restrict__ tw,
-                                                           const cplx<T>* __restrict__ work, T* __restrict__ phys) {
+__device__ __forceinline__ void bx_fill(cplx<T>* buf, const TransformDims& d, const cplx<T>* __restrict__ work,
+                                        int plane, int y0) {
   using C = cplx<T>;
   using PV = P2Vec<T>;
-  using R = typename PV::R;
-  constexpr int VW = PV::VW, RS = P2<L>::RS, NT = NB * L / 16, rows = 2 * NB;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  C* buf = reinterpret_cast<C*>(smem_raw);
-  const int plane = blockIdx.y;
-  const int y0 = blockIdx.x * rows;
+  constexpr int RS = P2<L>::RS, NT = NB * L / 16, rows = 2 * NB;
   constexpr int nxh = L / 3 * 2 / 2 + 1;   // d.nxh of a power-of-two Nx = L
   constexpr int gap = L - 2 * nxh + 1;  // FFT indices [nxh, L - nxh] are zero
   for (int idx = threadIdx.x; idx < NB * gap; idx += NT) {
@@ -679,6 +676,20 @@ __global__ void __launch_bounds__(NB * L / 16) bx_p2_kernel(TransformDims d, con
       }
     }
   }
+}
+
+template <typename T, int L, int NB>
+__global__ void __launch_bounds__(NB * L / 16) bx_p2_kernel(TransformDims d, const cplx<T>* __restrict__ tw,
+                                                           const cplx<T>* __restrict__ work, T* __restrict__ phys) {
+  using C = cplx<T>;
+  using PV = P2Vec<T>;
+  using R = typename PV::R;
+  constexpr int VW = PV::VW, RS = P2<L>::RS, NT = NB * L / 16, rows = 2 * NB;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* buf = reinterpret_cast<C*>(smem_raw);
+  const int plane = blockIdx.y;
+  const int y0 = blockIdx.x * rows;
+  bx_fill<T, L, NB>(buf, d, work, plane, y0);
   __syncthreads();
   ip_passes<T, +1, L, NB, 1>(buf, tw);
   T* dst = phys + (size_t)plane * d.ny * L;
@@ -697,6 +708,65 @@ __global__ void __launch_bounds__(NB * L / 16) bx_p2_kernel(TransformDims d, con
     }
     if (ya < d.ny) *reinterpret_cast<R*>(dst + (size_t)ya * L + x) = ra;
     if (yb < d.ny) *reinterpret_cast<R*>(dst + (size_t)yb * L + x) = rb;
+  }
+}
+
+// Backward x pass of ncomp groups of three gradient fields (work planes
+// (3c + j) * nz + z), each group reduced to the advection term
+//   out_c = (u + su) d_c/dx + (v + sv) d_c/dy + (w + sw) d_c/dz
+// of the advective nonlinear form (phase_carrier_flat.cc:786-797,
+// phase_scalar_flat.cc:588-591), so the nine physical gradient fields are
+// never written.  grid: (row blocks, nz, ncomp); unl: the physical velocity.
+// FP32: registers capped for about 640 threads per SM (measured best).
+template <typename T, int L, int NB>
+__global__ void __launch_bounds__(NB * L / 16, sizeof(T) == 4 ? 640 / (NB * L / 16) : 1) bx_adv_p2_kernel(TransformDims d, const cplx<T>* __restrict__ tw,
+                                                               const cplx<T>* __restrict__ work,
+                                                               const T* __restrict__ unl, T* __restrict__ out,
+                                                               size_t P, double su, double sv, double sw) {
+  using C = cplx<T>;
+  using PV = P2Vec<T>;
+  using R = typename PV::R;
+  constexpr int VW = PV::VW, RS = P2<L>::RS, NT = NB * L / 16, rows = 2 * NB;
+  constexpr int IS = NB * L / (NT * VW);
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* buf = reinterpret_cast<C*>(smem_raw);
+  const int z = blockIdx.y, c = blockIdx.z;
+  const int y0 = blockIdx.x * rows;
+  const size_t zoff = (size_t)z * d.ny * L;
+  R acca[IS], accb[IS];
+#pragma unroll
+  for (int i = 0; i < IS; ++i) acca[i] = accb[i] = vzero<R>();
+#pragma unroll 1
+  for (int j = 0; j < 3; ++j) {
+    if (j > 0) __syncthreads();   // buf is refilled
+    bx_fill<T, L, NB>(buf, d, work, (3 * c + j) * d.nz + z, y0);
+    __syncthreads();
+    ip_passes<T, +1, L, NB, 1>(buf, tw);
+    const T* uj = unl + (size_t)j * P + zoff;
+    const T sh = (T)(j == 0 ? su : j == 1 ? sv : sw);
+#pragma unroll
+    for (int i = 0; i < IS; ++i) {
+      const int e = (threadIdx.x + i * NT) * VW;
+      const int p = e / L, x = e % L;
+      const int ya = y0 + 2 * p, yb = ya + 1;
+      const R ua = ya < d.ny ? *reinterpret_cast<const R*>(uj + (size_t)ya * L + x) : vzero<R>();
+      const R ub = yb < d.ny ? *reinterpret_cast<const R*>(uj + (size_t)yb * L + x) : vzero<R>();
+#pragma unroll
+      for (int q = 0; q < VW; ++q) {
+        const C g = buf[p * RS + sp(x + q)];
+        vset(acca[i], q, vget(acca[i], q) + (vget(ua, q) + sh) * g.x);
+        vset(accb[i], q, vget(accb[i], q) + (vget(ub, q) + sh) * g.y);
+      }
+    }
+  }
+  T* dst = out + (size_t)c * P + zoff;
+#pragma unroll
+  for (int i = 0; i < IS; ++i) {
+    const int e = (threadIdx.x + i * NT) * VW;
+    const int p = e / L, x = e % L;
+    const int ya = y0 + 2 * p, yb = ya + 1;
+    if (ya < d.ny) *reinterpret_cast<R*>(dst + (size_t)ya * L + x) = acca[i];
+    if (yb < d.ny) *reinterpret_cast<R*>(dst + (size_t)yb * L + x) = accb[i];
   }
 }
 
@@ -915,8 +985,62 @@ template void dft_forward<double>(const TransformDims&, const FftPlan&, const Ff
                                   void*, cudaStream_t, const PhysProduct*);
 template void dft_forward<float>(const TransformDims&, const FftPlan&, const FftPlan&, const float*, double2*, int,
                                  void*, cudaStream_t, const PhysProduct*);
+template bool dft_backward_adv_ok<double>(const TransformDims&, const FftPlan&, const FftPlan&, const double*,
+                                          const double*);
+template bool dft_backward_adv_ok<float>(const TransformDims&, const FftPlan&, const FftPlan&, const float*,
+                                         const float*);
+template void dft_backward_adv<double>(const TransformDims&, const FftPlan&, const FftPlan&, const SpecGather&, int,
+                                       const double*, double*, double, double, double, void*, cudaStream_t);
+template void dft_backward_adv<float>(const TransformDims&, const FftPlan&, const FftPlan&, const SpecGather&, int,
+                                      const float*, float*, double, double, double, void*, cudaStream_t);
 template bool dft_forward_products_ok<double>(const TransformDims&, const FftPlan&, const PhysProduct&);
 template bool dft_forward_products_ok<float>(const TransformDims&, const FftPlan&, const PhysProduct&);
+template <typename T>
+bool dft_backward_adv_ok(const TransformDims& d, const FftPlan& px, const FftPlan& py, const T* unl, const T* out) {
+  return p2_length(px.L) && p2_length(py.L) && d.nxh == px.L / 3 * 2 / 2 + 1 && d.nyc == py.L / 3 * 2 &&
+         aligned16(unl) && aligned16(out) && ((size_t)d.nx * d.ny * d.nz * sizeof(T)) % 16 == 0;
+}
+
+template <typename T>
+void dft_backward_adv(const TransformDims& d, const FftPlan& px, const FftPlan& py, const SpecGather& grad, int ncomp,
+                      const T* unl, T* out, double su, double sv, double sw, void* work, cudaStream_t s) {
+  using C = cplx<T>;
+  if (ncomp < 1 || ncomp > 3 || grad.nf != 3 * ncomp || !dft_backward_adv_ok<T>(d, px, py, unl, out))
+    throw Error{TG_ERR_SHAPE, "RealCplxCube::DftBackward > advection on the x pass needs power-of-two Nx, Ny"};
+  C* w = reinterpret_cast<C*>(work);
+  const int planes = grad.nf * d.nz;
+  {  // y pass of the gradient fields, derivatives formed on load
+    prof_begin(s, PC_FFT_BY, (double)planes * ((double)d.nxh * d.ny * sizeof(C) + (double)d.M * sizeof(double2)), 0);
+    const C* tw = Tw<T>::get(py);
+    SpecGather gat = grad;
+#define TG_CALL(LL)                                                                                         \
+  {                                                                                                         \
+    constexpr int NB = P2Elems<T, P2_BY>::value / LL;                                                       \
+    dim3 grid((d.nxh + NB - 1) / NB, planes);                                                               \
+    by_p2_kernel<T, LL, NB, true><<<grid, NB * LL / 16, p2_smem<T, LL, P2_BY>(), s>>>(d, tw, nullptr, w, gat); \
+  }
+    TG_P2_DISPATCH(py.L, TG_CALL)
+#undef TG_CALL
+    prof_end(s);
+    TG_LAUNCH_CHECK("by_p2_kernel");
+  }
+  {  // x pass and the advection sums
+    const size_t P = (size_t)d.nx * d.ny * d.nz;
+    prof_begin(s, PC_FFT_BX, (double)ncomp * d.nz * d.ny * (3.0 * d.nxh * sizeof(C) + 4.0 * d.nx * sizeof(T)), 0);
+    const C* tw = Tw<T>::get(px);
+#define TG_CALL(LL)                                                                                  \
+  {                                                                                                  \
+    constexpr int NB = P2Elems<T, P2_BX>::value / LL;                                                \
+    dim3 grid((d.ny + 2 * NB - 1) / (2 * NB), d.nz, ncomp);                                          \
+    bx_adv_p2_kernel<T, LL, NB><<<grid, NB * LL / 16, p2_smem<T, LL, P2_BX>(), s>>>(d, tw, w, unl, out, P, su, sv, sw); \
+  }
+    TG_P2_DISPATCH(px.L, TG_CALL)
+#undef TG_CALL
+    prof_end(s);
+    TG_LAUNCH_CHECK("bx_adv_p2_kernel");
+  }
+}
+
 template void dft_backward<double>(const TransformDims&, const FftPlan&, const FftPlan&, const double2*, double*, int,
                                    void*, cudaStream_t, const SpecGather*);
 template void dft_backward<float>(const TransformDims&, const FftPlan&, const FftPlan&, const double2*, float*, int,

@@ -139,6 +139,15 @@ template <typename T>
 void dft_backward(const TransformDims& d, const FftPlan& px, const FftPlan& py,
                   const double2* spec, T* phys, int planes, void* work, cudaStream_t s,
                   const SpecGather* gather = nullptr);
+// Backward transforms of ncomp groups of three gradient fields (gathered
+// spectral sources, grad.nf = 3 ncomp, grad.plane0 = 0), each group reduced on
+// the x pass to out_c = (u+su) d_c/dx + (v+sv) d_c/dy + (w+sw) d_c/dz with the
+// physical velocity unl (3 fields); power-of-two Nx, Ny only (see _ok).
+template <typename T>
+bool dft_backward_adv_ok(const TransformDims& d, const FftPlan& px, const FftPlan& py, const T* unl, const T* out);
+template <typename T>
+void dft_backward_adv(const TransformDims& d, const FftPlan& px, const FftPlan& py, const SpecGather& grad, int ncomp,
+                      const T* unl, T* out, double su, double sv, double sw, void* work, cudaStream_t s);
 
 // ---------------------------------------------------------------------------
 // z-operator GEMM (gemm.cu):  out[r][m] = epi( sum_k A[r][k] in[k][m] )
