@@ -169,6 +169,19 @@ TG_API tg_status tg_run_steps(tg_ctx* ctx, int nsteps, int maxstep, double maxcf
  * kernel separately.  Results are identical either way.  Default: enabled.
  * (No reference counterpart; execution control.) */
 TG_API tg_status tg_set_graphs(tg_ctx* ctx, int enable);
+/* Row-tiling autotuner of the z-operator GEMMs (no reference counterpart: the
+ * reference's Armadillo products have no launch shape).  Times each distinct
+ * row tiling (output rows per CTA) of the dense and the folded product kernel
+ * on this grid and GPU, and applies the fastest to every operator of the
+ * context; results do not depend on the tiling.  cache_path (may be NULL): a
+ * JSON object {"<Nx>x<Ny>x<Nz>:<precision>:sm<cc>x<SMs>": [dense, folded]} of
+ * the two preferences (most 8-row m-tiles per CTA, 1-16 and 1-6); an entry for
+ * this case is applied without timing, a missing one is timed and added (the
+ * file is rewritten whole and renamed into place).  tiling (may be NULL)
+ * receives {m-tiles, row tiles} of the dense kernel then of the folded one.
+ * Call between steps: it waits for the context's streams, and the recorded
+ * step graphs are dropped. */
+TG_API tg_status tg_autotune(tg_ctx* ctx, const char* cache_path, int* tiling);
 /* tg_run_steps for n independent cases (each context on its own stream, e.g.
  * an ensemble of uneven grids and parameters): every case's step is enqueued
  * before any case's previous features are awaited, so the cases run

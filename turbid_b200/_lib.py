@@ -90,6 +90,7 @@ _SIGS = [
     ("tg_scalar_correct", _c_i, [_vp, _c_i]),
     ("tg_run_steps", _c_i, [_vp, _c_i, _c_i, _c_d, _pd, _pi]),
     ("tg_set_graphs", _c_i, [_vp, _c_i]),
+    ("tg_autotune", _c_i, [_vp, ctypes.c_char_p, _pi]),
     ("tg_swirling_strength", _c_i, [_vp, _pd]),
     ("tg_run_ensemble", _c_i, [ctypes.POINTER(ctypes.c_void_p), _c_i, _c_i, _c_i, _c_d, _pi]),
     ("tg_features", _c_i, [_vp, _pd]),

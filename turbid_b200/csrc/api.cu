@@ -9,11 +9,19 @@
 // results the reference never reads (only the bottom plane of du/dz, dv/dz
 // feeds the erosion flux; the scalar phase's physical velocity is the
 // carrier's plus a constant settling shift).
+#include <unistd.h>
+
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
+#include <fstream>
+#include <map>
 #include <memory>
+#include <regex>
+#include <sstream>
 #include <stdexcept>
+#include <string>
 
 #include "fields.cuh"
 #include "setup.h"
@@ -1111,6 +1119,194 @@ static void run_ensemble(std::vector<Ctx*>& xs, int nsteps, int maxstep, double 
   }
 }
 
+// ---------------------------------------------------------------------------
+// row-tiling autotuner of the z-operator GEMMs
+// ---------------------------------------------------------------------------
+// The row tiling (m-tiles of 8 output rows per CTA) sets how often each CTA
+// column re-reads its input from L2 against how evenly the grid fills the
+// SMs; the best choice depends on Nz, M and the GPU.  The tuner times the
+// store-epilogue product of three components for each distinct tiling of the
+// dense and the folded kernel and keeps the fastest; the choice is cached in a
+// flat JSON object {"<Nx>x<Ny>x<Nz>:<precision>:sm<cc>x<SMs>": [dense, folded]}
+// of the two preferences (most m-tiles per CTA).
+using TuneCache = std::map<std::string, std::pair<int, int>>;
+
+static std::string tune_key(const Ctx& x) {
+  int dev = 0;
+  TG_CUDA(cudaGetDevice(&dev));
+  int major = 0, minor = 0, sms = 0;
+  TG_CUDA(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev));
+  TG_CUDA(cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, dev));
+  TG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  char buf[128];
+  snprintf(buf, sizeof buf, "%dx%dx%d:%s:sm%d%dx%d", x.nx, x.ny, x.nz, x.mixed ? "mixed" : "fp64", major, minor,
+           sms);
+  return buf;
+}
+
+static TuneCache read_tune_cache(const char* path) {
+  TuneCache m;
+  std::ifstream f(path);
+  if (!f) return m;   // no cache yet
+  std::stringstream ss;
+  ss << f.rdbuf();
+  const std::string t = ss.str();
+  const size_t a = t.find_first_not_of(" \t\r\n"), b = t.find_last_not_of(" \t\r\n");
+  if (a != std::string::npos && (t[a] != '{' || t[b] != '}'))
+    throw Error{TG_ERR_ARG, std::string("tg_autotune > ") + path + " is not a tiling cache"};
+  static const std::regex entry("\"([^\"]+)\"\\s*:\\s*\\[\\s*(-?\\d+)\\s*,\\s*(-?\\d+)\\s*\\]");
+  for (std::sregex_iterator it(t.begin(), t.end(), entry), end; it != end; ++it)
+    m[(*it)[1].str()] = {std::stoi((*it)[2].str()), std::stoi((*it)[3].str())};
+  return m;
+}
+
+static void write_tune_cache(const char* path, const TuneCache& m) {
+  // whole file to a neighbour, then renamed over the cache: readers never
+  // see a partial file
+  const std::string tmp = std::string(path) + ".tmp" + std::to_string((long long)getpid());
+  {
+    std::ofstream f(tmp, std::ios::trunc);
+    if (!f) throw Error{TG_ERR_ARG, std::string("tg_autotune > cannot write ") + tmp};
+    f << "{\n";
+    size_t i = 0;
+    for (const auto& kv : m)
+      f << "  \"" << kv.first << "\": [" << kv.second.first << ", " << kv.second.second << "]"
+        << (++i < m.size() ? ",\n" : "\n");
+    f << "}\n";
+    if (!f) throw Error{TG_ERR_ARG, std::string("tg_autotune > cannot write ") + tmp};
+  }
+  if (std::rename(tmp.c_str(), path) != 0) {
+    std::remove(tmp.c_str());
+    throw Error{TG_ERR_ARG, std::string("tg_autotune > cannot write ") + path};
+  }
+}
+
+// device milliseconds of one launch: the least mean over three runs of five
+static float time_gemm(Ctx& x, const ZOperator& op, const double2* in, double2* out, int batch) {
+  cudaEvent_t a = nullptr, b = nullptr;
+  TG_CUDA(cudaEventCreate(&a));
+  TG_CUDA(cudaEventCreate(&b));
+  float best = 1e30f;
+  try {
+    for (int w = 0; w < 2; ++w) gemm(x, op, in, x.S, out, x.S, batch, EpiParams());
+    for (int r = 0; r < 3; ++r) {
+      TG_CUDA(cudaEventRecord(a, x.s));
+      for (int i = 0; i < 5; ++i) gemm(x, op, in, x.S, out, x.S, batch, EpiParams());
+      TG_CUDA(cudaEventRecord(b, x.s));
+      TG_CUDA(cudaEventSynchronize(b));
+      float ms = 0.f;
+      TG_CUDA(cudaEventElapsedTime(&ms, a, b));
+      best = std::min(best, ms / 5);
+    }
+  } catch (...) {
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    throw;
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  return best;
+}
+
+// distinct tilings of `rows` rows, from the fewest row tiles up
+static std::vector<int> tiling_candidates(int rows, int maxmt, int count) {
+  std::vector<int> prefs;
+  int last_tiles = -1;
+  for (int p = maxmt; p >= 1 && (int)prefs.size() < count; --p) {
+    int mt = 0, tiles = 0;
+    row_tiling(rows, p, mt, tiles);
+    if (tiles != last_tiles) prefs.push_back(p);
+    last_tiles = tiles;
+  }
+  return prefs;
+}
+
+static void apply_tiling(Ctx& x, int pd, int ps) {
+  zop_set_tiling(x.opD1, pd, ps);
+  zop_set_tiling(x.opD2, pd, ps);
+  zop_set_tiling(x.opTmp, pd, ps);
+  for (int i = 0; i < 5; ++i) {
+    zop_set_tiling(x.opEinv[i], pd, ps);
+    zop_set_tiling(x.opE[i], pd, ps);
+  }
+  x.drop_graphs();   // the recorded launches carry the old grids
+}
+
+static void autotune(Ctx& x, const char* cache_path, int* tiling) {
+  int maxd = 0, maxs = 0;
+  zop_tiling_limits(maxd, maxs);
+  const std::string key = tune_key(x);
+  TuneCache cache;
+  if (cache_path) cache = read_tune_cache(cache_path);
+  int pd = 0, ps = 0;
+  auto hit = cache.find(key);
+  if (hit != cache.end()) {
+    pd = hit->second.first;
+    ps = hit->second.second;
+    if (pd < 1 || pd > maxd || ps < 1 || ps > maxs)
+      throw Error{TG_ERR_ARG, "tg_autotune > cache entry " + key + " out of range"};
+  } else {
+    TG_CUDA(cudaStreamSynchronize(x.s));
+    if (x.s2) TG_CUDA(cudaStreamSynchronize(x.s2));
+    if (x.s3) TG_CUDA(cudaStreamSynchronize(x.s3));
+    Profiler* saved = g_prof;   // tuning launches stay out of a profiling window
+    g_prof = nullptr;
+    const size_t n = 3 * x.S;
+    double2 *in = nullptr, *out = nullptr;
+    cudaError_t e1 = cudaMalloc(&in, n * sizeof(double2));
+    cudaError_t e2 = cudaMalloc(&out, n * sizeof(double2));
+    try {
+      if (e1 != cudaSuccess || e2 != cudaSuccess) throw Error{TG_ERR_NOMEM, "tg_autotune > cudaMalloc"};
+      if (x.loaded)
+        TG_CUDA(cudaMemcpyAsync(in, x.U, n * sizeof(double2), cudaMemcpyDeviceToDevice, x.s));
+      else
+        TG_CUDA(cudaMemsetAsync(in, 0x3f, n * sizeof(double2), x.s));   // finite non-zero values
+      // the dense kernel on the dense copy of D1, the folded kernel on D1 itself
+      ZOperator dense = x.opD1, folded = x.opD1;
+      dense.sym = false;
+      dense.split = 0;
+      float best = 1e30f;
+      for (int p : tiling_candidates(x.nz, maxd, 6)) {
+        zop_set_tiling(dense, p, 0);
+        const float ms = time_gemm(x, dense, in, out, 3);
+        if (ms < best) best = ms, pd = p;
+      }
+      best = 1e30f;
+      if (folded.sym) {
+        for (int p : tiling_candidates(folded.rows, maxs, 4)) {
+          zop_set_tiling(folded, 0, p);
+          const float ms = time_gemm(x, folded, in, out, 3);
+          if (ms < best) best = ms, ps = p;
+        }
+      } else {
+        ps = maxs;   // no folded operator on this grid (even Nz)
+      }
+    } catch (...) {
+      cudaFree(in);
+      cudaFree(out);
+      g_prof = saved;
+      throw;
+    }
+    TG_CUDA(cudaFree(in));
+    TG_CUDA(cudaFree(out));
+    g_prof = saved;
+    if (cache_path) {
+      cache[key] = {pd, ps};
+      write_tune_cache(cache_path, cache);
+    }
+  }
+  apply_tiling(x, pd, ps);
+  if (tiling) {
+    int mt = 0, tiles = 0;
+    row_tiling(x.nz, pd, mt, tiles);
+    tiling[0] = mt;
+    tiling[1] = tiles;
+    row_tiling((x.nz - 1) / 2 + 1, ps, mt, tiles);
+    tiling[2] = mt;
+    tiling[3] = tiles;
+  }
+}
+
 }  // namespace tg
 
 // ===========================================================================
@@ -1413,6 +1609,11 @@ tg_status tg_set_graphs(tg_ctx* ctx, int enable) {
   x.graphs = enable != 0;
   if (!x.graphs) x.drop_graphs();
   return TG_OK;
+}
+
+tg_status tg_autotune(tg_ctx* ctx, const char* cache_path, int* tiling) {
+  TG_CHECK_CTX(ctx);
+  TG_TRY(autotune(*reinterpret_cast<Ctx*>(ctx), cache_path, tiling));
 }
 
 tg_status tg_run_ensemble(tg_ctx** ctxs, int n, int nsteps, int maxstep, double maxcfl, int* done) {

@@ -99,6 +99,10 @@ __device__ __forceinline__ EpiIn epi_load(const EpiParams& ep, int b, int r, int
   return in;
 }
 
+// Every rounding step of the epilogues is explicit (__fma_rn, __dmul_rn,
+// __dadd_rn): plain a * b + c may be fused or not by the code generator,
+// differently in each tile-shape instantiation, and the results are meant to be
+// bit-identical for every row tiling.
 template <int MODE>
 __device__ __forceinline__ double2 epi_apply(const EpiParams& ep, int b, int r, int m, double2 acc, const EpiIn& in) {
   switch (MODE) {
@@ -108,29 +112,31 @@ __device__ __forceinline__ double2 epi_apply(const EpiParams& ep, int b, int r, 
         R = 1.0 / in.s0;
         if (ep.null_mode && m == 0 && fabs(in.s1) < 10e-12) R = 0.0;
       }
-      return make_double2(acc.x * R, acc.y * R);
+      return make_double2(__dmul_rn(acc.x, R), __dmul_rn(acc.y, R));
     }
     case EPI_DIV: {
       const double2 x0 = in.a, x1 = in.c;
       const double kx = in.s0, ky = in.s1;
-      double re = (acc.x + (0.0 * x0.x - kx * x0.y)) + (0.0 * x1.x - ky * x1.y);
-      double im = (acc.y + (0.0 * x0.y + kx * x0.x)) + (0.0 * x1.y + ky * x1.x);
-      return make_double2(ep.s * re, ep.s * im);
+      const double re = __dadd_rn(__dadd_rn(acc.x, __fma_rn(-kx, x0.y, __dmul_rn(0.0, x0.x))),
+                                  __fma_rn(-ky, x1.y, __dmul_rn(0.0, x1.x)));
+      const double im = __dadd_rn(__dadd_rn(acc.y, __fma_rn(kx, x0.x, __dmul_rn(0.0, x0.y))),
+                                  __fma_rn(ky, x1.x, __dmul_rn(0.0, x1.y)));
+      return make_double2(__dmul_rn(ep.s, re), __dmul_rn(ep.s, im));
     }
     case EPI_LAPRHS: {
       const double2 h = in.a, u = in.c;
       const double dx2 = in.s0, dy2 = in.s1;
-      double lre = (acc.x + dx2 * u.x) + dy2 * u.x;
-      double lim = (acc.y + dx2 * u.y) + dy2 * u.y;
-      double ac2 = ep.a * ep.c2;
-      return make_double2((ac2 * h.x + ep.a * u.x) - lre, (ac2 * h.y + ep.a * u.y) - lim);
+      const double lre = __fma_rn(dy2, u.x, __fma_rn(dx2, u.x, acc.x));
+      const double lim = __fma_rn(dy2, u.y, __fma_rn(dx2, u.y, acc.y));
+      const double ac2 = __dmul_rn(ep.a, ep.c2);
+      return make_double2(__fma_rn(ac2, h.x, __fma_rn(ep.a, u.x, -lre)), __fma_rn(ac2, h.y, __fma_rn(ep.a, u.y, -lim)));
     }
     case EPI_GRAD: {
       const double2 x = in.a;
       const double kx = in.s0, ky = in.s1;
       const size_t oa = (size_t)b * ep.sAux + (size_t)r * ep.M + m;
-      ep.aux0[oa] = make_double2(0.0 * x.x - kx * x.y, 0.0 * x.y + kx * x.x);
-      ep.aux1[oa] = make_double2(0.0 * x.x - ky * x.y, 0.0 * x.y + ky * x.x);
+      ep.aux0[oa] = make_double2(__fma_rn(-kx, x.y, __dmul_rn(0.0, x.x)), __fma_rn(kx, x.x, __dmul_rn(0.0, x.y)));
+      ep.aux1[oa] = make_double2(__fma_rn(-ky, x.y, __dmul_rn(0.0, x.x)), __fma_rn(ky, x.x, __dmul_rn(0.0, x.y)));
       return acc;
     }
     default:
@@ -209,27 +215,26 @@ __device__ __forceinline__ void sym_store(const GemmArgs& g, int b, int r0, int 
     for (int half = 0; half < 2; ++half) {
       const int r = half == 0 ? i : (sp1 ? h + 1 + i : j);
       const bool row_ok = half == 0 ? i <= h : i < h;
-      EpiIn in[2];
-#pragma unroll
-      for (int nt = 0; nt < 2; ++nt)
-        if (row_ok && ok[nt]) in[nt] = epi_load<MODE>(g.ep, b, r, m[nt]);
+      // one n-tile at a time: the operand loads of both n-tiles at once
+      // spill the folded kernel's registers at MT = 6
 #pragma unroll
       for (int nt = 0; nt < 2; ++nt) {
         if (!(row_ok && ok[nt])) continue;
+        const EpiIn in = epi_load<MODE>(g.ep, b, r, m[nt]);
         const double pe = accE[mt][nt][0], pi = accE[mt][nt][1], qe = accO[mt][nt][0], qi = accO[mt][nt][1];
         double2 v;
         if (sp1)
           v = half == 0 ? make_double2(pe, pi) : make_double2(qe, qi);
         else if (half == 0)
-          v = make_double2(pe + qe, pi + qi);
+          v = make_double2(__dadd_rn(pe, qe), __dadd_rn(pi, qi));
         else {
-          v = make_double2(s * (pe - qe), s * (pi - qi));
+          v = make_double2(__dmul_rn(s, __dsub_rn(pe, qe)), __dmul_rn(s, __dsub_rn(pi, qi)));
           if (i == 0 && g.quirk != 0.0) {  // top row after the bottom one (x[0] = P + Q)
-            v.x += g.quirk * (pe + qe);
-            v.y += g.quirk * (pi + qi);
+            v.x = __fma_rn(g.quirk, __dadd_rn(pe, qe), v.x);
+            v.y = __fma_rn(g.quirk, __dadd_rn(pi, qi), v.y);
           }
         }
-        Cb[(size_t)r * g.M + m[nt]] = epi_apply<MODE>(g.ep, b, r, m[nt], v, in[nt]);
+        Cb[(size_t)r * g.M + m[nt]] = epi_apply<MODE>(g.ep, b, r, m[nt], v, in);
       }
     }
   }
@@ -503,6 +508,47 @@ void row_tiling(int rows, int maxmt, int& mt, int& tiles) {
   mt = (need + tiles - 1) / tiles;
 }
 
+// Rows of the padded operator buffers of an n x n operator: enough for every
+// tiling that a preference in [1, kMaxMtDense] (dense kernel, n rows) or
+// [1, kMaxMtSym] (folded kernel, h+1 rows) selects, so that re-tiling a built
+// operator needs no new buffers.
+static int rows_alloc(int n) {
+  const int hr = (n - 1) / 2 + 1;
+  int r = 0, mt = 0, tiles = 0;
+  for (int p = 1; p <= kMaxMtDense; ++p) {
+    row_tiling(n, p, mt, tiles);
+    r = std::max(r, mt * tiles * 8);
+  }
+  for (int p = 1; p <= kMaxMtSym; ++p) {
+    row_tiling(hr, p, mt, tiles);
+    r = std::max(r, mt * tiles * 8);
+  }
+  return r;
+}
+
+void zop_tiling_limits(int& max_dense, int& max_sym) {
+  max_dense = kMaxMtDense;
+  max_sym = kMaxMtSym;
+}
+
+void zop_set_tiling(ZOperator& op, int pref_dense, int pref_sym) {
+  if (pref_dense < 0 || pref_dense > kMaxMtDense || pref_sym < 0 || pref_sym > kMaxMtSym)
+    throw Error{TG_ERR_ARG, "zop_set_tiling > tiling out of range"};
+  op.pref_dense = pref_dense;
+  op.pref_sym = pref_sym;
+  if (op.n == 0) return;   // not built yet: zop_build applies the preferences
+  row_tiling(op.n, pref_dense ? pref_dense : kMaxMtDense, op.mt_dense, op.tiles_dense);
+  int need = op.mt_dense * op.tiles_dense * 8;
+  if (op.sym) {
+    row_tiling(op.rows, pref_sym ? pref_sym : kMaxMtSym, op.mt, op.tiles);
+    need = std::max(need, op.mt * op.tiles * 8);
+  } else {
+    op.mt = op.mt_dense;
+    op.tiles = op.tiles_dense;
+  }
+  if (op.rowsPad < need) throw Error{TG_ERR_ARG, "zop_set_tiling > operator buffer too small"};
+}
+
 static void zgemm_launch(const ZProblem* probs, int nprob, int M, cudaStream_t s);
 
 // Problems of one kernel shape share a launch; a group that mixes dense,
@@ -614,12 +660,12 @@ void zop_build(ZOperator& op, const std::vector<double>& A, int n, bool allow_sy
                const std::function<double*(size_t)>& alloc) {
   op.n = n;
   op.lda = (n + 15) / 16 * 16;
-  row_tiling(n, kMaxMtDense, op.mt_dense, op.tiles_dense);
+  row_tiling(n, op.pref_dense ? op.pref_dense : kMaxMtDense, op.mt_dense, op.tiles_dense);
   const int h = (n - 1) / 2;
   const int hr = h + 1;   // folded rows
   int mts, ts;
-  row_tiling(hr, kMaxMtSym, mts, ts);
-  const int rowsAlloc = std::max(op.tiles_dense * op.mt_dense * 8, ts * mts * 8);
+  row_tiling(hr, op.pref_sym ? op.pref_sym : kMaxMtSym, mts, ts);
+  const int rowsAlloc = rows_alloc(n);
   if (op.rowsPad == 0) op.rowsPad = rowsAlloc;
   if (op.rowsPad < rowsAlloc) throw Error{TG_ERR_ARG, "zop_build > operator buffer too small"};
   const size_t sz = (size_t)op.rowsPad * op.lda;
@@ -682,11 +728,11 @@ void zop_build_split(ZOperator& op, const std::vector<double>& A, int n, int spl
   if (!(n & 1) || n < 5 || (split != 1 && split != 2)) throw Error{TG_ERR_ARG, "zop_build_split > bad shape"};
   op.n = n;
   op.lda = (n + 15) / 16 * 16;
-  row_tiling(n, kMaxMtDense, op.mt_dense, op.tiles_dense);
+  row_tiling(n, op.pref_dense ? op.pref_dense : kMaxMtDense, op.mt_dense, op.tiles_dense);
   const int h = (n - 1) / 2, hr = h + 1;
   int mts, ts;
-  row_tiling(hr, kMaxMtSym, mts, ts);
-  const int rowsAlloc = std::max(op.tiles_dense * op.mt_dense * 8, ts * mts * 8);
+  row_tiling(hr, op.pref_sym ? op.pref_sym : kMaxMtSym, mts, ts);
+  const int rowsAlloc = rows_alloc(n);
   if (op.rowsPad == 0) op.rowsPad = rowsAlloc;
   if (op.rowsPad < rowsAlloc) throw Error{TG_ERR_ARG, "zop_build_split > operator buffer too small"};
   const size_t sz = (size_t)op.rowsPad * op.lda;

@@ -206,6 +206,9 @@ struct ZOperator {
   double quirk = 0.0;
   int rows = 0, mt = 0, tiles = 0;       // launch shape of the kernel used
   int mt_dense = 0, tiles_dense = 0;
+  // row-tile preferences (most m-tiles of 8 rows per CTA) of the dense and
+  // folded kernels; 0 = the built-in maximum
+  int pref_dense = 0, pref_sym = 0;
   double* A = nullptr;
   double* Ae = nullptr;
   double* Ao = nullptr;
@@ -230,6 +233,11 @@ void zop_build(ZOperator& op, const std::vector<double>& A, int n, bool allow_sy
 // halves of one step of a split Helmholtz solve (split = 1: Einvs, 2: Es)
 void zop_build_split(ZOperator& op, const std::vector<double>& A, int n, int split, double quirk,
                      const std::function<double*(size_t)>& alloc);
+// Re-tile an operator (built or not) for the row-tile preferences of the dense
+// and folded kernels (0 = built-in maximum); results do not depend on the
+// tiling, only the launch shape does.
+void zop_set_tiling(ZOperator& op, int pref_dense, int pref_sym);
+void zop_tiling_limits(int& max_dense, int& max_sym);
 void zgemm(const ZOperator& op, const double2* in, long long in_stride, double2* out, long long out_stride, int M,
            int batch, const EpiParams& ep, cudaStream_t s);
 // up to three problems whose operators share the kernel shape, in one launch

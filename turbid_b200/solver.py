@@ -9,6 +9,7 @@ reference's restart layout: complex (dim, Nxh, Nyc, Nz), z fastest.
 from __future__ import annotations
 
 import ctypes
+import os
 from typing import Optional, Tuple
 
 import numpy as np
@@ -123,6 +124,15 @@ class ChannelCase:
     def set_graphs(self, enable: bool):
         """Replay whole RK3 steps of run_steps as CUDA graphs (default) or not."""
         check(self.lib.tg_set_graphs(self.h, int(bool(enable))))
+
+    def autotune(self, cache_path: Optional[str] = None) -> dict:
+        """Pick the z-operator GEMM row tiling for this grid and GPU (timed, or
+        read from the JSON cache at cache_path) and apply it; returns the
+        m-tiles per CTA and row tiles of the dense and the folded kernel."""
+        t = (ctypes.c_int * 4)()
+        path = None if cache_path is None else os.fsencode(cache_path)
+        check(self.lib.tg_autotune(self.h, path, t))
+        return dict(mt_dense=t[0], tiles_dense=t[1], mt_folded=t[2], tiles_folded=t[3])
 
     def features(self) -> np.ndarray:
         f = np.zeros(_lib.TG_NFEATURE)
