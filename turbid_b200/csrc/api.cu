@@ -152,7 +152,10 @@ struct Ctx {
     void* p = nullptr;
     if (n == 0) n = 1;
     cudaError_t e = cudaMalloc(&p, n * sizeof(X));
-    if (e != cudaSuccess) throw Error{TG_ERR_NOMEM, std::string("tg_create > cudaMalloc > ") + cudaGetErrorString(e)};
+    if (e != cudaSuccess) {
+      (void)cudaGetLastError();   // not left for the next launch check
+      throw Error{TG_ERR_NOMEM, std::string("tg_create > cudaMalloc > ") + cudaGetErrorString(e)};
+    }
     allocs.push_back(p);
     TG_CUDA(cudaMemset(p, 0, n * sizeof(X)));
     return reinterpret_cast<X*>(p);
@@ -1256,7 +1259,10 @@ static void autotune(Ctx& x, const char* cache_path, int* tiling) {
     cudaError_t e1 = cudaMalloc(&in, n * sizeof(double2));
     cudaError_t e2 = cudaMalloc(&out, n * sizeof(double2));
     try {
-      if (e1 != cudaSuccess || e2 != cudaSuccess) throw Error{TG_ERR_NOMEM, "tg_autotune > cudaMalloc"};
+      if (e1 != cudaSuccess || e2 != cudaSuccess) {
+        (void)cudaGetLastError();   // not left for the next launch check
+        throw Error{TG_ERR_NOMEM, "tg_autotune > cudaMalloc"};
+      }
       if (x.loaded)
         TG_CUDA(cudaMemcpyAsync(in, x.U, n * sizeof(double2), cudaMemcpyDeviceToDevice, x.s));
       else

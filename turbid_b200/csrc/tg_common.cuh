@@ -20,12 +20,17 @@ struct Error {
   std::string msg;
 };
 
+// A failed runtime call also records its error as the thread's last error;
+// a non-sticky one (out of memory, invalid argument) is cleared here, so that
+// the next TG_LAUNCH_CHECK does not report it against an unrelated launch.
 #define TG_CUDA(call)                                                           \
   do {                                                                          \
     cudaError_t e_ = (call);                                                    \
-    if (e_ != cudaSuccess)                                                      \
+    if (e_ != cudaSuccess) {                                                    \
+      (void)cudaGetLastError();                                                 \
       throw ::tg::Error{TG_ERR_CUDA, std::string(#call) + " > " +               \
                                          cudaGetErrorString(e_)};               \
+    }                                                                           \
   } while (0)
 
 extern long long g_launches;   // kernel launches issued by this library (host thread count)
