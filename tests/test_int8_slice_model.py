@@ -1,0 +1,124 @@
+"""CPU model of an FP64 z-operator product assembled from exact int8 slice
+products (Ozaki-style splitting: Ozaki, Ogita, Oishi, Rump, "Error-free
+transformations of matrix multiplication", Numer. Algorithms 2012, with integer
+slices as in Ootomo, Ozaki, Yokota, "DGEMM on integer matrix multiplication
+unit", 2024), on the 257-point Chebyshev operators of the 256x256x257 case.
+
+The operator A is split by rows and the data X by columns into s slices of
+signed integers of at most 64 in magnitude, each row / column scaled by a power
+of two: the first slice holds 6 bits, every further one 7.  The products of
+slices p and q are exact in int32 (|sum| <= 64 * 64 * 257) and are summed in
+FP64 with weight 2^-(6+7p) 2^-(6+7q), over p + q < s.  Here the exact integer
+products are formed with FP64 matrix products (every partial sum is an integer
+below 2^53) and compared with a long-double product.
+
+The tests pin how many slices each operator of the step needs: the Helmholtz
+solve chain E (R .* (E^-1 X)) (src/phase_carrier_flat.cc:861-994) reaches
+FP64's own error at 8 slices and 1e-9 at 5; the second-derivative operator D2
+(src/stepper_space_chebyshev.cc:101-228), whose products cancel by about four
+orders of magnitude, needs 8 slices for 1e-11 (plain FP64: 7e-13).
+"""
+import math
+
+import numpy as np
+import pytest
+
+from oracle import turbid_oracle as O
+
+NZ = 257
+
+
+def split(M, axis, s):
+    mx = np.max(np.abs(M), axis=axis, keepdims=True)
+    e = np.ceil(np.log2(np.where(mx > 0, mx, 1.0)))
+    r = M / 2.0 ** e
+    slices = []
+    q = np.rint(r * 64)
+    slices.append(q)
+    r = r * 64 - q
+    for _ in range(1, s):
+        q = np.rint(r * 128)
+        slices.append(q)
+        r = r * 128 - q
+    for q in slices:
+        assert np.max(np.abs(q)) <= 64
+    return slices, 2.0 ** e
+
+
+def sliced_product(A, X, s):
+    As, ea = split(A, 1, s)
+    Xs, ex = split(X, 0, s)
+    C = np.zeros((A.shape[0], X.shape[1]))
+    for p in range(s):
+        for q in range(s - p):
+            P = As[p] @ Xs[q]
+            assert np.max(np.abs(P)) < 2 ** 31          # fits the int32 accumulator
+            C += P * 2.0 ** (-(6 + 7 * p) - (6 + 7 * q))
+    return C * ea * ex
+
+
+def exact(A, X):
+    return A.astype(np.longdouble) @ X.astype(np.longdouble)
+
+
+def rel(a, b):
+    b = np.asarray(b, dtype=np.float64)
+    return float(np.linalg.norm(np.asarray(a, dtype=np.float64) - b) / np.linalg.norm(b))
+
+
+@pytest.fixture(scope="module")
+def setup():
+    cfg = O.CaseConfig(nx=24, ny=24, nz=NZ, reynolds=800.0, dt=2 * math.pi / 2000, bc_u=[1, 0, 0, 1, 0])
+    g = O.Grid(cfg)
+    D1, D2 = O.chebyshev_d1_d2(g)
+    sc = [-cfg.reynolds / cfg.dt / O.RK3[2, s] for s in range(3)]
+    dec = O.Dz2Decomposition(g, D1, D2, cfg.bc_u, sc)
+    # columns: resolved Chebyshev series (coefficients decaying to 1e-13 over the
+    # 257 modes, amplitudes over six decades) plus a Stokes wall layer
+    rng = np.random.default_rng(11)
+    z = g.gridz
+    k = np.arange(NZ)
+    T = np.cos(np.outer(np.arccos(np.clip(z, -1, 1)), k))
+    cols = []
+    delta = math.sqrt(2 / cfg.reynolds)
+    for _ in range(64):
+        a = rng.standard_normal(NZ) * np.exp(-k * math.log(1e13) / (NZ - 1)) * 10.0 ** rng.uniform(-6, 0)
+        cols.append(T @ a + rng.uniform() * np.exp(-(z + 1) / delta) * np.cos((z + 1) / delta))
+    X = np.stack(cols, axis=1)
+    R = dec.R[0][: X.shape[1]].T          # (Nz, columns): reciprocal of stage 1, one column per mode
+    return D1, D2, dec.E, dec.Einv, R, X
+
+
+def errors(fn, ref):
+    return {s: rel(fn(s), ref) for s in range(4, 9)}
+
+
+def test_slices_gain_seven_bits_each(setup):
+    D1, D2, E, Ei, R, X = setup
+    for A in (D1, D2, E, Ei):
+        err = errors(lambda s: sliced_product(A, X, s), exact(A, X))
+        for s in range(4, 8):
+            floor = 1e-15 if A is not D2 else 1e-13
+            if err[s + 1] > floor:
+                assert err[s] / err[s + 1] > 30, (s, err)
+
+
+def test_solve_chain_slice_counts(setup):
+    _, _, E, Ei, R, X = setup
+    X = X.copy()
+    X[0] = X[-1] = 0.0    # boundary rows are the fix rows' work (E, R are the identity there)
+    ref = exact(E, R.astype(np.longdouble) * exact(Ei, X))   # the whole chain in long double
+    fp64 = rel(E @ (R * (Ei @ X)), ref)
+    err = errors(lambda s: sliced_product(E, R * sliced_product(Ei, X, s), s), ref)
+    assert err[5] < 1e-8          # mixed mode budget (fields within 1e-5 after 100 steps)
+    assert err[8] < 1e-14 and err[8] < 20 * fp64   # FP64 mode: at FP64's own level
+
+
+def test_derivative_slice_counts(setup):
+    D1, D2, _, _, _, X = setup
+    e1 = errors(lambda s: sliced_product(D1, X, s), exact(D1, X))
+    e2 = errors(lambda s: sliced_product(D2, X, s), exact(D2, X))
+    f2 = rel(D2 @ X, exact(D2, X))
+    assert e1[6] < 1e-8 and e1[8] < 1e-12
+    assert e2[7] < 1e-8 and e2[8] < 1e-10
+    assert f2 < e2[8]             # plain FP64 D2 stays ahead of 8 slices
