@@ -330,6 +330,9 @@ def our_arm(args):
     case = tb.ChannelCase(**dict(params, precision=prec))
     case.set_stream(stream.cuda_stream)
     case.upload_state(uvw0, p0, phi0)
+    # z-operator GEMM row tiling picked by the library's own autotuner (timed
+    # here, before the warm-up; the fields do not depend on it)
+    tiling = case.autotune(None)
     case.run_steps(args.warmup)
     barrier()
 
@@ -477,7 +480,9 @@ def our_arm(args):
             "data": "synthetic (seeded Stokes profile + divergence-free perturbation, 10% scalar noise)",
             "config": {"workload": f"{args.workload} {wdesc(args.workload)}", "precision": prec,
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                       "l2": "inputs larger than L2 (no flush)"},
+                       "l2": "inputs larger than L2 (no flush)",
+                       "gemm_tiling": "autotuned: dense {mt_dense} m-tiles x {tiles_dense} row tiles, "
+                                      "folded {mt_folded} x {tiles_folded}".format(**tiling)},
             "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks, "roofline": roof,
             "cpu_baseline": cpu, "accuracy_vs_fp64_gpu": acc, "fp64_gpu_steps_per_s": fp64_rate,
             "kernels": kernels,
