@@ -34,6 +34,33 @@ def test_library_exports_every_declared_symbol():
     assert lib.tg_version() >= 1
 
 
+# entry points that take a context and check it before any CUDA call
+CTX_ENTRY_POINTS = ["tg_get_dims", "tg_set_stream", "tg_synchronize", "tg_get_operators", "tg_upload_state",
+                    "tg_download_state", "tg_set_time", "tg_carrier_predict", "tg_carrier_correct",
+                    "tg_swirling_strength", "tg_set_graphs", "tg_autotune", "tg_run_steps", "tg_profile_begin",
+                    "tg_profile_end", "tg_profile_executed", "tg_features", "tg_dft_forward_f64",
+                    "tg_dft_forward_f32", "tg_dft_backward_f64", "tg_dft_backward_f32", "tg_multiply",
+                    "tg_helmholtz"]
+
+
+@pytest.mark.parametrize("name", CTX_ENTRY_POINTS)
+def test_null_context_is_refused(name):
+    """A null context returns TG_ERR_ARG with a message, no GPU touched."""
+    import ctypes
+    lib = _lib.load()
+    fn = getattr(lib, name)
+    args = []
+    for t in fn.argtypes:
+        if t in (ctypes.c_int, ctypes.c_longlong):
+            args.append(1)
+        elif t is ctypes.c_double:
+            args.append(0.0)
+        else:
+            args.append(None)
+    assert fn(*args) == 3
+    assert b"null context" in lib.tg_last_error()
+
+
 @pytest.mark.parametrize("nz,mapping,coef", [(17, 0, 0.0), (65, 0, 0.0), (33, 1, 0.7), (33, 2, 0.9), (33, 3, 0.8)])
 def test_host_operators_match_oracle(nz, mapping, coef):
     cfg = O.CaseConfig(nx=4, ny=4, nz=nz, mapping=mapping, mapping_coef=coef)
