@@ -16,7 +16,11 @@ The tests pin how many slices each operator of the step needs: the Helmholtz
 solve chain E (R .* (E^-1 X)) (src/phase_carrier_flat.cc:861-994) reaches
 FP64's own error at 8 slices and 1e-9 at 5; the second-derivative operator D2
 (src/stepper_space_chebyshev.cc:101-228), whose products cancel by about four
-orders of magnitude, needs 8 slices for 1e-11 (plain FP64: 7e-13).
+orders of magnitude, needs 8 slices for 1e-11 (plain FP64: 7e-13).  Through
+the whole RK3 step (the oracle's products replaced): the two boundary rows of
+the data must be applied exactly (the scalar's Robin rows carry 1e7-scaled
+values), and then 6 slices everywhere (or 5 for the solves with D1, D2 in
+FP64) meet the mixed mode's budget and 8 the FP64 mode's.
 """
 import math
 
@@ -122,3 +126,101 @@ def test_derivative_slice_counts(setup):
     assert e1[6] < 1e-8 and e1[8] < 1e-12
     assert e2[7] < 1e-8 and e2[8] < 1e-10
     assert f2 < e2[8]             # plain FP64 D2 stays ahead of 8 slices
+
+
+
+def make_sliced_zmul(s, exact_rows=True, skip=()):
+    """The oracle's z-operator product (zmul) through s-slice products.  With
+    exact_rows the two boundary rows of the data (z = -1, 1) are applied as an
+    exact FP64 rank-2 update and only the interior rows are sliced (their
+    scale then ignores boundary values: the scalar's Robin rows are scaled by
+    1e7, src/common.h:55).  Operators in `skip` stay plain FP64."""
+    cache = {}
+
+    def zmul(A, X):
+        if any(A is k for k in skip):
+            return ORIG_ZMUL(A, X)
+        hit = cache.get(id(A))
+        if hit is None or hit[0] is not A:
+            Ai = A.copy()
+            if exact_rows:
+                Ai[:, 0] = Ai[:, -1] = 0.0
+            hit = cache[id(A)] = (A, split(Ai, 1, s))
+        As, ea = hit[1]
+        R = np.stack([X.real, X.imag])
+        cols = R.reshape(-1, R.shape[-1]).T.copy()            # (Nz, columns): one z-profile per column
+        bottom, top = cols[0].copy(), cols[-1].copy()
+        if exact_rows:
+            cols[0] = cols[-1] = 0.0
+        Xs, ex = split(cols, 0, s)
+        C = np.zeros((A.shape[0], cols.shape[1]))
+        for p in range(s):
+            for q in range(s - p):
+                C += (As[p] @ Xs[q]) * 2.0 ** (-(6 + 7 * p) - (6 + 7 * q))
+        C *= ea * ex
+        if exact_rows:
+            C += np.outer(A[:, 0], bottom) + np.outer(A[:, -1], top)
+        Y = C.T.reshape(R.shape)
+        return Y[0] + 1j * Y[1]
+
+    return zmul
+
+
+ORIG_ZMUL = O.zmul
+
+
+def sediment_case():
+    return O.CaseConfig(nx=16, ny=16, nz=NZ, nphase=2, reynolds=800.0, froude=1.0, averaged_concentration=1e-3,
+                        specific_gravity=2.65, bc_u=[1, 0, 0, 1, 0], bc_v=[1, 0, 0, 1, 0], settling=5e-4,
+                        schmidt=0.5, critical_shear=2e-4, erosion_rate=1e-4, dt=2 * math.pi / 2000)
+
+
+def field_error(sol, ref):
+    return max(O.rel_l2(sol.uvw, ref.uvw), O.rel_l2(sol.p, ref.p), O.rel_l2(sol.phi, ref.phi))
+
+
+def test_robin_rows_need_exact_boundary_rows(monkeypatch):
+    """The scalar solve's data carry the 1e7-scaled Robin rows: scaled with
+    them, the interior rows of E_s's product lose about 23 bits."""
+    cfg = sediment_case()
+    uvw, p, phi = O.make_initial_state(cfg, seed=3, noise=0.05)
+    sol = O.OracleSolver(cfg, uvw, p, phi)
+    worst = {True: 0.0, False: 0.0}
+    variants = {k: make_sliced_zmul(6, exact_rows=k) for k in worst}
+
+    def probe(A, X):
+        y = ORIG_ZMUL(A, X)
+        if A is sol.dec_s.E:
+            for k, fn in variants.items():
+                ys = fn(A, X)
+                e = np.linalg.norm(ys[..., 1:-1] - y[..., 1:-1]) / np.linalg.norm(y[..., 1:-1])
+                worst[k] = max(worst[k], e)
+        return y
+
+    monkeypatch.setattr(O, "zmul", probe)
+    sol.run_step()
+    assert worst[False] > 1e-4 and worst[True] < 1e-9, worst
+
+
+def test_solver_with_sliced_products(monkeypatch):
+    """20 RK3 steps of the 16x16x257 sediment case with the z-operator products
+    through s slices (exact boundary rows), against the FP64 oracle: every
+    product at 6 slices meets the mixed budget, at 8 the FP64 one; with D1 and
+    D2 kept in FP64 the solves need only 5 slices for the mixed budget."""
+    cfg = sediment_case()
+    uvw, p, phi = O.make_initial_state(cfg, seed=3, noise=0.05)
+    nsteps = 20
+    ref = O.OracleSolver(cfg, uvw, p, phi)
+    for _ in range(nsteps):
+        ref.run_step()
+    err = {}
+    for key, s, deriv_fp64 in (("all6", 6, False), ("all8", 8, False), ("solves5", 5, True)):
+        sol = O.OracleSolver(cfg, uvw, p, phi)
+        with monkeypatch.context() as m:
+            m.setattr(O, "zmul", make_sliced_zmul(s, skip=(sol.D1, sol.D2) if deriv_fp64 else ()))
+            for _ in range(nsteps):
+                sol.run_step()
+        err[key] = field_error(sol, ref)
+    assert err["all6"] < 1e-6, err
+    assert err["all8"] < 1e-9, err
+    assert err["solves5"] < 2e-6, err
