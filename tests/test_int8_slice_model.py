@@ -33,8 +33,13 @@ NZ = 257
 
 
 def split(M, axis, s):
+    """s slices and the power-of-two scales: |M / scale| <= 1 with scale the
+    least power of two at or above the row / column maximum (frexp: exact, no
+    floating logarithm); every step below is exact in FP64 (power-of-two
+    scalings, and the difference of a value and its nearest integer)."""
     mx = np.max(np.abs(M), axis=axis, keepdims=True)
-    e = np.ceil(np.log2(np.where(mx > 0, mx, 1.0)))
+    f, e = np.frexp(np.where(mx > 0, mx, 1.0))        # mx = f 2^e, f in [0.5, 1)
+    e = np.where(f == 0.5, e - 1, e).astype(np.float64)
     r = M / 2.0 ** e
     slices = []
     q = np.rint(r * 64)
@@ -47,6 +52,21 @@ def split(M, axis, s):
     for q in slices:
         assert np.max(np.abs(q)) <= 64
     return slices, 2.0 ** e
+
+
+def test_split_is_exact_to_its_last_slice():
+    rng = np.random.default_rng(5)
+    X = rng.standard_normal((NZ, 40)) * 10.0 ** rng.uniform(-8, 8, 40)
+    X[:, 0] = 2.0 ** -3                                   # exact powers of two keep their exponent
+    for s in (1, 3, 5, 8):
+        Xs, ex = split(X, 0, s)
+        back = sum(q * 2.0 ** (-(6 + 7 * p)) for p, q in enumerate(Xs)) * ex
+        # half a unit of the last slice, plus the rounding of the FP64 sum above
+        # (eight slices span 55 bits)
+        bound = 2.0 ** (-(6 + 7 * (s - 1)) - 1) * ex + 2.0 ** -52 * np.abs(X)
+        assert np.all(np.abs(back - X) <= bound)
+        assert np.all(np.abs(X / ex) <= 1.0)
+    assert ex[0, 0] == 2.0 ** -3
 
 
 def sliced_product(A, X, s):
