@@ -7,8 +7,9 @@ unit", 2024), on the 257-point Chebyshev operators of the 256x256x257 case.
 The operator A is split by rows and the data X by columns into s slices of
 signed integers of at most 64 in magnitude, each row / column scaled by a power
 of two: the first slice holds 6 bits, every further one 7.  The products of
-slices p and q are exact in int32 (|sum| <= 64 * 64 * 257) and are summed in
-FP64 with weight 2^-(6+7p) 2^-(6+7q), over p + q < s.  Here the exact integer
+slices p and q are exact in int32 (|sum| <= 64 * 64 * 257 per pair, at most s
+pairs per diagonal p + q); each diagonal is summed exactly and the diagonals
+in FP64 with weight 2^-(12+7(p+q)), over p + q < s.  Here the exact integer
 products are formed with FP64 matrix products (every partial sum is an integer
 below 2^53) and compared with a long-double product.
 
@@ -69,16 +70,22 @@ def test_split_is_exact_to_its_last_slice():
     assert ex[0, 0] == 2.0 ** -3
 
 
+def combine(As, Xs, s):
+    """Sum over the slice pairs p + q < s as the tensor-core kernel does: the
+    pairs of one diagonal d = p + q summed exactly (one int32 accumulator per
+    diagonal), then the diagonals in FP64 with weight 2^-(12+7d), d ascending."""
+    C = np.zeros((As[0].shape[0], Xs[0].shape[1]))
+    for d in range(s):
+        Dd = sum(As[p] @ Xs[d - p] for p in range(d + 1))   # exact: integers below 2^53
+        assert np.max(np.abs(Dd)) < 2 ** 31                  # fits the int32 accumulator
+        C = Dd * 2.0 ** (-(12 + 7 * d)) + C
+    return C
+
+
 def sliced_product(A, X, s):
     As, ea = split(A, 1, s)
     Xs, ex = split(X, 0, s)
-    C = np.zeros((A.shape[0], X.shape[1]))
-    for p in range(s):
-        for q in range(s - p):
-            P = As[p] @ Xs[q]
-            assert np.max(np.abs(P)) < 2 ** 31          # fits the int32 accumulator
-            C += P * 2.0 ** (-(6 + 7 * p) - (6 + 7 * q))
-    return C * ea * ex
+    return combine(As, Xs, s) * ea * ex
 
 
 def exact(A, X):
@@ -173,11 +180,7 @@ def make_sliced_zmul(s, exact_rows=True, skip=()):
         if exact_rows:
             cols[0] = cols[-1] = 0.0
         Xs, ex = split(cols, 0, s)
-        C = np.zeros((A.shape[0], cols.shape[1]))
-        for p in range(s):
-            for q in range(s - p):
-                C += (As[p] @ Xs[q]) * 2.0 ** (-(6 + 7 * p) - (6 + 7 * q))
-        C *= ea * ex
+        C = combine(As, Xs, s) * ea * ex
         if exact_rows:
             C += np.outer(A[:, 0], bottom) + np.outer(A[:, -1], top)
         Y = C.T.reshape(R.shape)
