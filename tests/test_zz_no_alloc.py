@@ -1,9 +1,11 @@
 """GPU check of tg_dft_forward_f64_noalloc, the allocation-free forward
 transform for callers that manage all device memory themselves and must not
-have the library call cudaMalloc.  Its output must equal the context-based
-tg_dft_forward_f64 (same kernels and twiddles) on two calls in a row, the
-second with a different grid, since both calls share the library's static
-scratch array.  Kept in its own file so that it is collected last.
+have the library call cudaMalloc.  Its output must agree with the
+context-based tg_dft_forward_f64 (the same pruned transform, other radix
+passes) to 1e-13 relative L2 on two calls in a row, the second with a
+different grid, since both calls share the library's static scratch array;
+the second call is also checked against the oracle's numpy transform.  Kept
+in its own file so that it is collected last.
 """
 import ctypes
 
@@ -11,6 +13,7 @@ import numpy as np
 import pytest
 
 import turbid_b200 as tb
+from oracle import turbid_oracle as O
 from turbid_b200 import _lib
 
 pytestmark = pytest.mark.gpu
@@ -44,6 +47,10 @@ def test_noalloc_forward_matches_context_forward(cuda, calls):
         assert np.isfinite(a).all()
         err = np.linalg.norm((a - b).ravel()) / np.linalg.norm(b.ravel())
         assert err < 1e-13, (nx, ny, nz, dim, err)
+    # the last call against the oracle (numpy rfft/fft, pruned, scaled 1/(Nx Ny))
+    g = O.Grid(O.CaseConfig(nx=nx, ny=ny, nz=nz))
+    ref_np = O.dft_forward(g, x.cpu().numpy())
+    assert O.rel_l2(tb.from_slab(a, g.nxh, g.nyc), ref_np) < 1e-13
 
 
 def test_noalloc_forward_rejects_unsupported_sizes(cuda):

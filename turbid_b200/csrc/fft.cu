@@ -19,6 +19,8 @@
 #include <cstring>
 #include <mutex>
 
+#include <cuda.h>
+
 #include "fft_dev.cuh"
 
 namespace tg {
@@ -1070,6 +1072,7 @@ __device__ __align__(256) int g_noalloc_yidx[kNoAllocTable];
 
 struct NoAllocDevice {
   bool ready = false;
+  unsigned long long ctx_id = 0;   // context the tables were written in (0: unknown)
   double2* scratch = nullptr;
   double2* tw = nullptr;
   int* yidx = nullptr;
@@ -1083,16 +1086,48 @@ inline int noalloc_offset(int L) { return L - kNoAllocMinL; }
 
 bool is_supported_pow2(int L) { return L >= kNoAllocMinL && L <= kNoAllocMaxL && (L & (L - 1)) == 0; }
 
+// Unique id of the calling thread's current CUDA context (cuCtxGetId through
+// the runtime's driver entry points, so the library does not link libcuda), or
+// 0 when there is none yet or the driver does not offer the call.
+unsigned long long current_context_id() {
+  typedef CUresult (*GetCurrentFn)(CUcontext*);
+  typedef CUresult (*GetIdFn)(CUcontext, unsigned long long*);
+  static GetCurrentFn get_current = nullptr;
+  static GetIdFn get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = reinterpret_cast<GetCurrentFn>(f);
+    f = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<GetIdFn>(f);
+    (void)cudaGetLastError();
+  });
+  if (!get_current || !get_id) return 0;
+  CUcontext c = nullptr;
+  unsigned long long id = 0;
+  if (get_current(&c) != CUDA_SUCCESS || !c || get_id(c, &id) != CUDA_SUCCESS) return 0;
+  return id;
+}
+
 // Per-device set-up, run by the first call on each device (device current).
 // The table copies are synchronous host->device copies, which a stream capture
 // does not allow: the first call on a device must come before any capture.
+// A reset of the device (cudaDeviceReset, or the primary context released and
+// created again) wipes the device arrays and their addresses; the set-up is
+// repeated when the current context is not the one it ran in.
 NoAllocDevice& noalloc_setup() {
   int dev = 0;
   TG_CUDA(cudaGetDevice(&dev));
   if (dev < 0 || dev >= kNoAllocMaxDevices) throw Error{TG_ERR_ARG, "tg_dft_forward_f64_noalloc > device index out of range"};
   std::lock_guard<std::mutex> lock(g_noalloc_mu);
   NoAllocDevice& d = g_noalloc_dev[dev];
-  if (d.ready) return d;
+  if (d.ready && d.ctx_id == current_context_id()) return d;
+  d.ready = false;
   std::vector<double2> tw(kNoAllocTable, make_double2(0.0, 0.0));
   std::vector<int> ym(kNoAllocTable, 0);
   for (int L = kNoAllocMinL; L <= kNoAllocMaxL; L *= 2) {
@@ -1113,6 +1148,7 @@ NoAllocDevice& noalloc_setup() {
 #define TG_INIT_L(L) set_smem_all<double, L>();
   TG_FFT_LENGTHS(TG_INIT_L)
 #undef TG_INIT_L
+  d.ctx_id = current_context_id();   // the copies above made the context current
   d.ready = true;
   return d;
 }
