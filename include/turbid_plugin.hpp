@@ -213,6 +213,10 @@ class IniFile {
     while (in >> tok) v.push_back(Expression::Evaluate(tok));
     return v;
   }
+  bool HasKey(const std::string& sec, const std::string& key) const {
+    auto s = sections_.find(sec);
+    return s != sections_.end() && s->second.count(key) != 0;
+  }
   std::vector<int> GetVectorInt(const std::string& sec, const std::string& key) const {
     std::istringstream in(GetValueString(sec, key));
     std::vector<int> v;
@@ -577,12 +581,13 @@ class FlatVariables {
 class FlatChannelSolver {
  public:
   // argv[1]: configuration file (default configuration.ini), argv[2]: log
-  // file (default logcomputation); --mixed selects mixed precision.
+  // file (default logcomputation); --mixed selects mixed precision, as does
+  // gpu_precision = Mixed in the file's [System] section.
   FlatChannelSolver(int argc, char** argv) {
     std::vector<std::string> pos;
     for (int i = 1; i < argc; ++i) {
       const std::string a = argv[i];
-      if (a == "--mixed") precision_ = TG_PREC_MIXED;
+      if (a == "--mixed") mixed_flag_ = true;
       else pos.push_back(a);
     }
     if (pos.size() > 0) config_ = pos[0];
@@ -592,6 +597,13 @@ class FlatChannelSolver {
   }
   void Configure() {
     ini_.Load(config_);
+    precision_ = TG_PREC_FP64;
+    if (ini_.HasKey("System", "gpu_precision")) {
+      const std::string pr = Upper(ini_.GetValueString("System", "gpu_precision"));
+      if (pr == "MIXED") precision_ = TG_PREC_MIXED;
+      else if (pr != "FP64") throw std::runtime_error("FlatChannelSolver::Configure > gpu_precision must be FP64 or Mixed");
+    }
+    if (mixed_flag_) precision_ = TG_PREC_MIXED;
     const tg_case c = CaseFromIni(ini_, rc_, precision_);
     gpu_.reset(new GpuCase(c));
     carrier_.reset(new FlatCarrierPhase(*gpu_));
@@ -611,7 +623,8 @@ class FlatChannelSolver {
   void Execute() {
     if (!configured_) throw std::runtime_error("FlatChannelSolver::Execute > Not Configured!");
     std::ofstream log(directory_ + logname_, std::ios::app);
-    std::vector<double> feature = carrier_->GetFeatureGlobal();
+    std::vector<double>& feature = feature_;
+    feature = carrier_->GetFeatureGlobal();
     while (tstepper_.isForward()) {
       // a CFL above the limit (or the last step) clears the forward flag; the
       // step is still taken and, with the output flag, written for record.
@@ -645,6 +658,30 @@ class FlatChannelSolver {
     Check("FlatChannelSolver::Execute", tg_synchronize(gpu_->ctx()));
   }
 
+  // Case summary written before the first log line: grid, precision, time
+  // stepping and the physical parameters (the reference prints its component
+  // objects there, src/solver_channel_flat.cc:340-366).
+  void PrintLogHead(std::ostream& s) const {
+    const std::string sep(80, '*');
+    s << sep << "\n";
+    if (gpu_) {
+      const tg_case& c = gpu_->config();
+      s << std::setw(30) << std::right << "FlatChannelSolver > " << "grid " << c.nx << " x " << c.ny << " x " << c.nz
+        << ", phases " << c.nphase << ", precision " << (c.precision == TG_PREC_MIXED ? "Mixed" : "FP64") << "\n";
+      s << std::setw(30) << std::right << "RK3TimeStepper > " << std::setprecision(10) << "dt " << tstepper_.GetTimeStep()
+        << ", start step " << tstepper_.GetStep() << ", max step " << rc_.maxstep << ", max cfl " << rc_.maxcfl << "\n";
+      s << std::setw(30) << std::right << "FlatCarrierPhase > " << "Re " << c.reynolds << ", force type " << c.force_type
+        << "\n";
+      if (c.nphase > 1)
+        s << std::setw(30) << std::right << "FlatScalarPhase > " << "Sc " << c.schmidt << ", Ws " << c.settling
+          << ", boundary " << (c.scalar_bc ? "ErosionDeposition" : "ZeroFlux") << "\n";
+    }
+    s << sep << "\n";
+  }
+  // The last step's log line (the features read after that step).
+  void PrintLogBody(std::ostream& s) const { PrintLogBody(s, feature_); }
+  const std::vector<double>& Features() const { return feature_; }
+
   // FlatChannelSolver::PrintLogBody (src/solver_channel_flat.cc:372-414)
   void PrintLogBody(std::ostream& s, const std::vector<double>& f) const {
     s << std::setw(12) << tstepper_.GetStep() << std::setw(16) << std::setprecision(10) << tstepper_.GetTime()
@@ -657,7 +694,9 @@ class FlatChannelSolver {
  private:
   std::string config_ = "configuration.ini", logname_ = "logcomputation", directory_ = "./";
   int precision_ = TG_PREC_FP64;
+  bool mixed_flag_ = false;
   bool configured_ = false;
+  std::vector<double> feature_ = std::vector<double>(TG_NFEATURE, 0.0);
   IniFile ini_;
   RunControl rc_;
   RK3TimeStepper tstepper_;
