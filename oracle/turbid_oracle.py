@@ -517,13 +517,14 @@ def stokes_profile(re: float, z: np.ndarray, t: float, free_slip_top: bool = Fal
 
 
 def make_initial_state(cfg: CaseConfig, seed: int = 0, noise: float = 1e-4,
-                       scalar_noise: float = 0.1, modes: int = 3):
+                       scalar_noise: float = 0.1, modes: int = 3, scalar_mean=1.0):
     """Seeded synthetic restart state (spectral uvw (3,..), p (1,..), phi (1,..)).
 
     Mean mode: the analytic laminar profile at t = 0.  Perturbation: the curl of a
     seeded vector potential with wall-vanishing envelope (1 - z^2)^2 and Fourier
     modes |kx|,|ky| <= `modes`, scaled so that its peak equals `noise`.  phi is
-    1 + `scalar_noise` * uniform(-1, 1) noise, mean mode set to 1.
+    `scalar_mean` + `scalar_noise` * uniform(-1, 1) noise, mean mode set to
+    `scalar_mean` (a number, or one value per z plane).
     """
     g = Grid(cfg)
     rng = np.random.default_rng(seed)
@@ -563,9 +564,10 @@ def make_initial_state(cfg: CaseConfig, seed: int = 0, noise: float = 1e-4,
         prof[-1] = 0.0
     uvw[0, 0, 0, :] += prof
     p = np.zeros((1, g.nxh, g.nyc, g.nz), dtype=np.complex128)
-    phi_phys = 1.0 + scalar_noise * rng.uniform(-1.0, 1.0, size=(1, g.nz, g.ny, g.nx))
+    mean = np.broadcast_to(np.asarray(scalar_mean, dtype=np.float64), (g.nz,))
+    phi_phys = mean[None, :, None, None] + scalar_noise * rng.uniform(-1.0, 1.0, size=(1, g.nz, g.ny, g.nx))
     phi = dft_forward(g, phi_phys)
-    phi[0, 0, 0, :] = 1.0
+    phi[0, 0, 0, :] = mean
     return uvw, p, phi
 
 

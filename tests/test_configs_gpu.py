@@ -1,0 +1,110 @@
+"""GPU runs of the benchmark configurations' correctness checks, through the
+library's own operators and decompositions (the path the bench and the main
+programs run), against the FP64 oracle.
+
+* 32x32x65 laminar oscillatory Stokes layer, Re_delta = 180, no sediment,
+  no-slip bottom and free-slip top, dt = 2 pi/2000, 500 RK3 steps: the
+  plane-averaged u against the analytic solution (tmtools/get_loflow.m:17-20,
+  RMS metric of examples/oscillatory_flow_re180_laminar/mcode/e_analysis.m:
+  54-58) and every field against the oracle.
+* 128x128x129, Re_delta = 800 with the sediment scalar, FP64: the oracle's
+  steps (2-3 s each on 8 host cores) bound the comparison to four steps;
+  the GPU then runs on to 200 steps and the state stays finite and bounded.
+* Nz = 257 (the benchmark's Chebyshev grid), FP64, a few steps against the
+  oracle.
+Tolerance: 1e-10 relative L2 per field against the oracle.
+"""
+import math
+
+import numpy as np
+import pytest
+
+import turbid_b200 as tb
+from oracle import turbid_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+KEYS = ("nx", "ny", "nz", "lx", "ly", "nphase", "mapping", "mapping_coef", "slope", "slope_direction", "dt",
+        "output_based_on_step", "reynolds", "froude", "averaged_concentration", "specific_gravity",
+        "affected_by_scalar", "bc_u", "bc_v", "bc_w", "bc_p", "force_type", "force_direction",
+        "force_amplitude", "schmidt", "settling", "erosion_rate", "critical_shear", "scalar_bc")
+TOL = 1e-10
+
+
+def sediment(nx, ny, nz, re=800.0):
+    return O.CaseConfig(nx=nx, ny=ny, nz=nz, nphase=2, lx=4 * math.pi, ly=2 * math.pi, reynolds=re, froude=1.0,
+                        averaged_concentration=1e-3, specific_gravity=2.65, bc_u=[1, 0, 0, 1, 0],
+                        bc_v=[1, 0, 0, 1, 0], settling=5e-4, schmidt=0.5, critical_shear=2e-4, erosion_rate=1e-4,
+                        dt=2 * math.pi / 2000)
+
+
+def fields(u, p, c):
+    out = {"u": u[0], "v": u[1], "w": u[2], "p": p[0]}
+    if c is not None:
+        out["c"] = c[0]
+    return out
+
+
+def compare(gc, sol, tol):
+    gu, gp, gc_ = gc.download_state()
+    got = fields(gu, gp, gc_)
+    ref = fields(sol.uvw, sol.p, sol.phi if sol.scalar else None)
+    errs = {k: O.rel_l2(got[k], ref[k]) for k in ref}
+    assert max(errs.values()) < tol, errs
+    return errs
+
+
+def test_cfg1_laminar_stokes_500_steps(cuda):
+    cfg = O.CaseConfig(nx=32, ny=32, nz=65, lx=4 * math.pi, ly=2 * math.pi, reynolds=180.0,
+                       dt=2 * math.pi / 2000, bc_u=[1, 0, 0, 1, 0], bc_v=[1, 0, 0, 1, 0])
+    uvw, p, _ = O.make_initial_state(cfg, seed=1, noise=1e-4)
+    gc = tb.ChannelCase(precision="fp64", **{k: getattr(cfg, k) for k in KEYS})
+    gc.upload_state(uvw, p, None)
+    assert gc.run_steps(500) == 500
+    sol = O.OracleSolver(cfg, uvw, p)
+    for _ in range(500):
+        sol.run_step()
+    compare(gc, sol, TOL)
+    t = gc.get_time()
+    assert t["step"] == 500 and abs(t["time"] - sol.time) < 1e-12
+    gu, _, _ = gc.download_state()
+    mu = O.dft_backward(sol.g, gu[:1])[0].mean(axis=(1, 2))
+    ua = O.stokes_profile(180.0, sol.g.gridz, sol.time, free_slip_top=True)
+    rms = np.sqrt(np.mean((mu - ua) ** 2))
+    assert rms < 1e-6, rms          # the oracle's own error here is 4.5e-7 (dt and the 1e-4 perturbation)
+    gc.close()
+
+
+def test_cfg2_fp64_128_sediment(cuda):
+    cfg = sediment(128, 128, 129)
+    uvw, p, phi = O.make_initial_state(cfg, seed=2, noise=0.05)
+    gc = tb.ChannelCase(precision="fp64", **{k: getattr(cfg, k) for k in KEYS})
+    gc.upload_state(uvw, p, phi)
+    sol = O.OracleSolver(cfg, uvw, p, phi)
+    for _ in range(4):   # both nonlinear forms, twice
+        sol.run_step()
+        assert gc.run_steps(1) == 1
+    compare(gc, sol, TOL)
+    feats = np.zeros(50)
+    assert gc.run_steps(196, features=feats) == 196
+    gu, gp, gphi = gc.download_state()
+    assert np.isfinite(gu).all() and np.isfinite(gp).all() and np.isfinite(gphi).all()
+    assert 0.1 < feats[0] < 3.0          # max |u| of the driven layer stays O(1)
+    gc.close()
+
+
+@pytest.mark.parametrize("nphase", [1, 2])
+def test_fp64_steps_nz257(cuda, nphase):
+    cfg = sediment(16, 16, 257)
+    if nphase == 1:
+        cfg.nphase = 1
+    uvw, p, phi = O.make_initial_state(cfg, seed=3, noise=0.05)
+    phi = phi if nphase == 2 else None
+    gc = tb.ChannelCase(precision="fp64", **{k: getattr(cfg, k) for k in KEYS})
+    gc.upload_state(uvw, p, phi)
+    sol = O.OracleSolver(cfg, uvw, p, phi)
+    for _ in range(3):
+        sol.run_step()
+    assert gc.run_steps(3) == 3
+    compare(gc, sol, TOL)
+    gc.close()

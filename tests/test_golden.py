@@ -7,7 +7,7 @@ RK3 steps, started from the stored state, reproduce the stored results.
 
 Tolerances (relative L2 per field): oracle rerun 1e-12; host operators 1e-13;
 host decomposition action 1e-10; GPU transform 1e-13; GPU RK3 steps 1e-10 with
-the stored decompositions, 1e-9 with the library's own.
+the stored decompositions and with the library's own.
 """
 import json
 import math
@@ -123,7 +123,7 @@ def test_golden_steps_gpu(cuda, name, stored_dec):
     if stored_dec:
         for w in range(5 if scalar else 4):
             gc.set_decomposition(w, *[z[f"dec{w}_{k}"] for k in ("E", "Einv", "lam", "fbb", "ftb", "fbf", "ftf")])
-    tol = 1e-10 if stored_dec else 1e-9
+    tol = 1e-10
     gc.upload_state(z["uvw0"], z["p0"], z["phi0"] if scalar else None)
     feats = np.zeros(50)
     for k in range(1, 4):

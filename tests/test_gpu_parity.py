@@ -141,8 +141,8 @@ def test_helmholtz_matches_oracle(cuda):
 # ----------------------------------------------------------------------------
 # RK3 steps
 # ----------------------------------------------------------------------------
-def _compare_run(cfg, nsteps, seed, noise, tol, oracle_dec=True, check_features=True):
-    uvw, p, phi = O.make_initial_state(cfg, seed=seed, noise=noise)
+def _compare_run(cfg, nsteps, seed, noise, tol, oracle_dec=True, check_features=True, **state_kw):
+    uvw, p, phi = O.make_initial_state(cfg, seed=seed, noise=noise, **state_kw)
     sol = O.OracleSolver(cfg, uvw, p, phi if cfg.nphase > 1 else None)
     gc = gpu_case(cfg)
     if oracle_dec:
@@ -200,9 +200,40 @@ def test_fp64_steps_radix16_transforms(cuda):
     _compare_run(sediment_cfg(nx=64, ny=64, nz=17), 2, seed=9, noise=0.05, tol=1e-10)
 
 
+def filter_active_state_kw(nz):
+    """A scalar whose physical values cross zero (mean 0.05, +-0.1 noise) and
+    whose mean is negative on two planes: the Bartnicki filter redistributes
+    on every plane and zeroes whole planes (phase_scalar_flat.cc:419-478)."""
+    mean = np.full(nz, 0.05)
+    mean[4] = -0.03
+    mean[11] = -0.02
+    return dict(scalar_mean=mean, scalar_noise=0.1)
+
+
+def test_fp64_steps_positivity_filter_active(cuda):
+    cfg = sediment_cfg(nx=16, ny=12, nz=17)
+    _compare_run(cfg, 3, seed=13, noise=0.05, tol=1e-10, **filter_active_state_kw(cfg.nz))
+
+
+def test_mixed_positivity_filter_active_close_to_fp64(cuda):
+    """The FP32 filter of the mixed mode on the same zero-crossing scalar."""
+    cfg = sediment_cfg(nx=32, ny=32, nz=17)
+    uvw, p, phi = O.make_initial_state(cfg, seed=13, noise=0.05, **filter_active_state_kw(cfg.nz))
+    f64 = gpu_case(cfg, "fp64")
+    mx = gpu_case(cfg, "mixed")
+    for c in (f64, mx):
+        c.upload_state(uvw, p, phi)
+        c.run_steps(5)
+    u1, p1, c1 = f64.download_state()
+    u2, p2, c2 = mx.download_state()
+    assert rel(c2, c1) < 1e-5 and rel(u2, u1) < 1e-5 and rel(p2, p1) < 1e-5
+    f64.close()
+    mx.close()
+
+
 def test_fp64_steps_native_decompositions(cuda):
     """Operators built by the library's own eigen-solver (no oracle matrices)."""
-    _compare_run(sediment_cfg(nz=33), 3, seed=6, noise=0.05, tol=1e-9, oracle_dec=False, check_features=False)
+    _compare_run(sediment_cfg(nz=33), 3, seed=6, noise=0.05, tol=1e-10, oracle_dec=False, check_features=False)
 
 
 def test_plugin_methods_match_run_steps(cuda):

@@ -547,6 +547,11 @@ void positivity_filter(T* phip, int plane_n, int nz, cudaStream_t s) {
 // Stage-2 features of FlatCarrierPhase::Correct (phase_carrier_flat.cc:633-703).
 // bits: 10 slots of non-negative doubles reduced with atomicMax on their bit
 // patterns: 0-2 max|u_i|, 3-5 bottom plane, 6-8 top plane, 9 max CFL length.
+// The maxima keep a NaN (fmax would drop it; a positive NaN's bit pattern is
+// above +inf's, so atomicMax keeps it too): a non-finite velocity anywhere
+// reaches the features, where the host's guard reports it.
+__device__ __forceinline__ double max_keep_nan(double a, double b) { return (b > a || isnan(b)) ? b : a; }
+
 template <typename T>
 __global__ void k_feature_max(const T* __restrict__ unl, int nx, int ny, int nz, const double* __restrict__ glz,
                               double lmx, double lmy, unsigned long long* bits) {
@@ -558,15 +563,15 @@ __global__ void k_feature_max(const T* __restrict__ unl, int nx, int ny, int nz,
   double mu = 0, mv = 0, mw = 0, ml = 0;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < plane; i += (size_t)gridDim.x * blockDim.x) {
     const double u = fabs((double)pu[i]), v = fabs((double)pu[P + i]), w = fabs((double)pu[2 * P + i]);
-    mu = fmax(mu, u);
-    mv = fmax(mv, v);
-    mw = fmax(mw, w);
-    ml = fmax(ml, u / lmx + v / lmy + w / gl);
+    mu = max_keep_nan(mu, u);
+    mv = max_keep_nan(mv, v);
+    mw = max_keep_nan(mw, w);
+    ml = max_keep_nan(ml, u / lmx + v / lmy + w / gl);
   }
   double mx[4] = {mu, mv, mw, ml};
 #pragma unroll
   for (int k = 0; k < 4; ++k)
-    for (int o = 16; o > 0; o >>= 1) mx[k] = fmax(mx[k], __shfl_down_sync(0xffffffffu, mx[k], o));
+    for (int o = 16; o > 0; o >>= 1) mx[k] = max_keep_nan(mx[k], __shfl_down_sync(0xffffffffu, mx[k], o));
   // block maximum first: one atomic per block and value (the values are
   // non-negative, so their bit patterns order like the numbers)
   __shared__ double wm[32][4];
@@ -576,7 +581,9 @@ __global__ void k_feature_max(const T* __restrict__ unl, int nx, int ny, int nz,
   __syncthreads();
   if (threadIdx.x == 0) {
     for (int w = 1; w < nw; ++w)
-      for (int k = 0; k < 4; ++k) mx[k] = fmax(mx[k], wm[w][k]);
+      for (int k = 0; k < 4; ++k) mx[k] = max_keep_nan(mx[k], wm[w][k]);
+    for (int k = 0; k < 4; ++k)   // a NaN of either sign becomes the positive quiet NaN
+      if (isnan(mx[k])) mx[k] = __longlong_as_double(0x7ff8000000000000LL);
     for (int k = 0; k < 3; ++k) {
       const unsigned long long b = (unsigned long long)__double_as_longlong(mx[k]);
       atomicMax(bits + k, b);
