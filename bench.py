@@ -276,7 +276,8 @@ def reference_arm(args):
     rate, done, el, setup = cpu_step_rate(args.workload, args.steps, args.cpu_budget, args.warmup)
     line = {
         "impl": "reference", "metric": METRIC, "value": rate, "unit": "steps/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / rate, "higher_is_better": True,
+        "steps": done, "steps_requested": args.steps, "warmup": min(args.warmup, 1), "ms_per_step": 1e3 / rate,
+        "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": f"{args.workload} " + wdesc(args.workload), "precision": "fp64 (CPU)"},
         "cpu_baseline": {"value": rate, "unit": "steps/s", "cores": cores, "kind": "port",
@@ -329,6 +330,8 @@ def our_arm(args):
     stream = torch.cuda.Stream()
     case = tb.ChannelCase(**dict(params, precision=prec))
     case.set_stream(stream.cuda_stream)
+    if args.zsolver and prec == "mixed":
+        case.set_zsolver(args.zsolver)
     case.upload_state(uvw0, p0, phi0)
     # z-operator GEMM row tiling picked by the library's own autotuner (timed
     # here, before the warm-up; the fields do not depend on it)
@@ -391,7 +394,7 @@ def our_arm(args):
     # ---- accuracy vs the FP64 GPU path + FP64 GPU rate (same seed, same steps)
     acc = None
     fp64_rate = None
-    if prec == "mixed" and not args.skip_accuracy:
+    if prec == "mixed" and not args.skip_accuracy and args.acc_steps > 0:
         ref = tb.ChannelCase(**dict(params, precision="fp64"))
         ref.set_stream(stream.cuda_stream)
         ref.upload_state(uvw0, p0, phi0)
@@ -455,6 +458,9 @@ def our_arm(args):
         gbs = v["bytes"] / (v["ms"] * 1e-3) / 1e9 if v["ms"] > 0 else 0.0
         ent = {"ms_per_step": v["ms"] / steps_p, "launches_per_step": v["count"] / steps_p, "GB/s": gbs,
                "hbm_frac": gbs / hbm}
+        tr = traffic_summary().get(args.workload, {}).get(prec, {}).get(k)
+        if tr:
+            ent["traffic_per_launch"] = tr
         if v["flops"]:
             ent["TFLOP/s"] = v["flops"] / (v["ms"] * 1e-3) / 1e12
             ent["executed_TFLOP/s"] = v.get("xflops", v["flops"]) / (v["ms"] * 1e-3) / 1e12
@@ -481,6 +487,7 @@ def our_arm(args):
             "config": {"workload": f"{args.workload} {wdesc(args.workload)}", "precision": prec,
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                        "l2": "inputs larger than L2 (no flush)",
+                       "zsolver": (args.zsolver or "library default") if prec == "mixed" else "dmma",
                        "gemm_tiling": "autotuned: dense {mt_dense} m-tiles x {tiles_dense} row tiles, "
                                       "folded {mt_folded} x {tiles_folded}".format(**tiling)},
             "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks, "roofline": roof,
@@ -501,12 +508,17 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="cfg3", choices=sorted(WORKLOADS))
     ap.add_argument("--precision", default=None, choices=[None, "fp64", "mixed"])
+    ap.add_argument("--zsolver", default=None, choices=[None, "dmma", "islice"],
+                    help="products of the dense Helmholtz solves in mixed precision (default: the library's)")
     ap.add_argument("--prof-steps", type=int, default=3)
-    ap.add_argument("--acc-steps", type=int, default=100)
+    ap.add_argument("--acc-steps", type=int, default=None,
+                    help="steps of the mixed vs FP64 comparison (default 100; 5 for cfg5)")
     ap.add_argument("--skip-accuracy", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=60.0)
     args = ap.parse_args()
+    if args.acc_steps is None:
+        args.acc_steps = 5 if args.workload == "cfg5" else 100
     if args.impl == "reference":
         reference_arm(args)
     elif args.workload == "cfg4":

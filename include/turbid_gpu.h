@@ -238,9 +238,19 @@ TG_API tg_status tg_dft_forward_f32(tg_ctx* ctx, const float* phys, double* spec
  * start at zero: each call writes every scratch element before reading it.
  * All calls share the one scratch array: calls whose work overlaps on the GPU
  * (other streams or other host threads) race; order them on one stream.
- * Results equal tg_dft_forward_f64's. */
+ * A device reset after the first call is followed by the set-up again on the
+ * next call.  Results agree with tg_dft_forward_f64's to rounding (about 1e-13
+ * relative L2): the same pruned transform, evaluated here with radix-4 and
+ * radix-2 passes where the context path uses radix-16 passes. */
 TG_API tg_status tg_dft_forward_f64_noalloc(int nx, int ny, int nz, const double* phys,
                                             double* spec, int dim, void* stream);
+/* The same transforms over any number of z planes (physical planes of Ny x Nx
+ * in, spectral planes of M out, or back): the local x and y passes of one
+ * rank's z-slab in a slab/column decomposition over several GPUs, as P3DFFT
+ * does them before its z exchange (build/ftran.F90:50-263,
+ * build/btran.F90:48-257).  fp32 != 0: FP32 physical planes. */
+TG_API tg_status tg_dft_forward_planes(tg_ctx* ctx, const void* phys, double* spec, int planes, int fp32);
+TG_API tg_status tg_dft_backward_planes(tg_ctx* ctx, const double* spec, void* phys, int planes, int fp32);
 /* RealCplxCube::DftBackward (src/cube_real_cplx.cc:542-555): zero-fill, unscaled. */
 TG_API tg_status tg_dft_backward_f64(tg_ctx* ctx, const double* spec, double* phys, int dim);
 TG_API tg_status tg_dft_backward_f32(tg_ctx* ctx, const double* spec, float* phys, int dim);
@@ -249,6 +259,26 @@ TG_API tg_status tg_dft_backward_f32(tg_ctx* ctx, const double* spec, float* phy
  * memory (copied to the device on each call). */
 TG_API tg_status tg_multiply(tg_ctx* ctx, const double* A_host, const double* in,
                       double* out, int dim);
+/* RealCplxCube::Multiply (src/cube_real_cplx.cc:461-471) through the
+ * int8-slice tensor-core product that the mixed precision mode uses for its
+ * dense Helmholtz solves: A and in split into 5 exact int8 slices over the
+ * interior rows (z = 1 .. nz-2), the slice products exact in int32 on the
+ * tcgen05 tensor cores, combined in FP64, the two boundary rows added in FP64.
+ * Relative error about 1e-9 of the FP64 product; nz <= 258.  Same arguments
+ * as tg_multiply. */
+TG_API tg_status tg_multiply_islice(tg_ctx* ctx, const double* A_host, const double* in, double* out, int dim);
+/* z-solver of the dense Helmholtz solves (u, v and the scalar) in mixed
+ * precision (no reference counterpart; execution control):
+ * TG_ZSOLVER_DMMA = FP64 tensor-core products, TG_ZSOLVER_ISLICE = the
+ * int8-slice product of tg_multiply_islice (default in mixed precision).
+ * FP64 precision always uses TG_ZSOLVER_DMMA.  Recorded step graphs are
+ * dropped. */
+#define TG_ZSOLVER_DMMA   0
+#define TG_ZSOLVER_ISLICE 1
+TG_API tg_status tg_set_zsolver(tg_ctx* ctx, int solver);
+/* 1 in *flag when a bounded device wait of an int8-slice product gave up
+ * since the context was created (the product's output is then invalid). */
+TG_API tg_status tg_zsolver_error(tg_ctx* ctx, int* flag);
 /* CmDz2 solve of FlatCarrierPhase::Helmholtz / FlatScalarPhase::Helmholtz
  * (src/phase_carrier_flat.cc:861-994, src/phase_scalar_flat.cc:635-667) for
  * one spectral component: which as in tg_set_decomposition, stage 0..2;

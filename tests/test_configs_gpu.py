@@ -12,7 +12,16 @@ programs run), against the FP64 oracle.
   the GPU then runs on to 200 steps and the state stays finite and bounded.
 * Nz = 257 (the benchmark's Chebyshev grid), FP64, a few steps against the
   oracle.
-Tolerance: 1e-10 relative L2 per field against the oracle.
+Tolerance: 1e-10 relative L2 per field against the oracle, except the
+laminar case's pressure after 500 steps.  There the pressure is a small
+field (|p| / |u| about 2e-7, driven only by the 1e-4 perturbation) and its
+relative error at 500 steps is set by the choice of eigenvectors in the
+decompositions: the oracle itself, run once with numpy's eigenvectors and
+once with the same eigenvectors rescaled by random factors in [0.5, 2] (an
+equally valid decomposition with the same solve operator to rounding),
+differs by 1.4e-10 in p (1.7e-11 at 100 steps) while u, v, w agree to 5e-13.
+The reference's own eigen-solver (Armadillo eig_gen on MKL) is another such
+choice, so that case's pressure is held to 5e-10.
 """
 import math
 
@@ -45,12 +54,13 @@ def fields(u, p, c):
     return out
 
 
-def compare(gc, sol, tol):
+def compare(gc, sol, tol, tol_p=None):
     gu, gp, gc_ = gc.download_state()
     got = fields(gu, gp, gc_)
     ref = fields(sol.uvw, sol.p, sol.phi if sol.scalar else None)
     errs = {k: O.rel_l2(got[k], ref[k]) for k in ref}
-    assert max(errs.values()) < tol, errs
+    for k, e in errs.items():
+        assert e < (tol_p if k == "p" and tol_p else tol), errs
     return errs
 
 
@@ -64,7 +74,7 @@ def test_cfg1_laminar_stokes_500_steps(cuda):
     sol = O.OracleSolver(cfg, uvw, p)
     for _ in range(500):
         sol.run_step()
-    compare(gc, sol, TOL)
+    compare(gc, sol, TOL, tol_p=5e-10)
     t = gc.get_time()
     assert t["step"] == 500 and abs(t["time"] - sol.time) < 1e-12
     gu, _, _ = gc.download_state()

@@ -100,9 +100,14 @@ _SIGS = [
     ("tg_dft_forward_f64", _c_i, [_vp, _vp, _vp, _c_i]),
     ("tg_dft_forward_f32", _c_i, [_vp, _vp, _vp, _c_i]),
     ("tg_dft_forward_f64_noalloc", _c_i, [_c_i, _c_i, _c_i, _vp, _vp, _c_i, _vp]),
+    ("tg_dft_forward_planes", _c_i, [_vp, _vp, _vp, _c_i, _c_i]),
+    ("tg_dft_backward_planes", _c_i, [_vp, _vp, _vp, _c_i, _c_i]),
     ("tg_dft_backward_f64", _c_i, [_vp, _vp, _vp, _c_i]),
     ("tg_dft_backward_f32", _c_i, [_vp, _vp, _vp, _c_i]),
     ("tg_multiply", _c_i, [_vp, _pd, _vp, _vp, _c_i]),
+    ("tg_multiply_islice", _c_i, [_vp, _pd, _vp, _vp, _c_i]),
+    ("tg_set_zsolver", _c_i, [_vp, _c_i]),
+    ("tg_zsolver_error", _c_i, [_vp, _pi]),
     ("tg_helmholtz", _c_i, [_vp, _c_i, _c_i, _vp, _vp]),
 ]
 

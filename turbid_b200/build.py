@@ -18,9 +18,17 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libturbid_gpu.so")
 BUILD_DIR = os.path.join(HERE, "_build")
 
-CU_SOURCES = ["api.cu", "fft.cu", "gemm.cu", "fields.cu"]
+CU_SOURCES = ["api.cu", "fft.cu", "gemm.cu", "fields.cu", "islice.cu"]
 DRIVER_SRC = os.path.join(HERE, "host", "channelflat_gpu.cc")
 DRIVER = os.path.join(HERE, "channelflat_gpu")
+# the reference's solver-layer library (include/solver_channel_flat.h)
+PSLIB_SRC = os.path.join(HERE, "host", "pseudospectral.cc")
+PSLIB = os.path.join(HERE, "libpseudospectral.so")
+# the reference's own main program, compiled unchanged against PSLIB when a
+# reference source tree is at hand (built here, not committed; it travels with
+# the other built files)
+REFERENCE = os.environ.get("TURBID_REFERENCE", "/root/reference")
+REF_MAIN = os.path.join(HERE, "channelflat")
 INCLUDE = os.path.join(HERE, "..", "include")
 CC_SOURCES = ["setup.cc"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -47,6 +55,7 @@ def build(verbose: bool = False, force: bool = False) -> str:
     headers.append(os.path.join(HERE, "..", "include", "turbid_gpu.h"))
     if not force and _newer(LIB, srcs + headers):
         build_driver(verbose=verbose)
+        build_pseudospectral(verbose=verbose)
         return LIB
     os.makedirs(BUILD_DIR, exist_ok=True)
     nvcc = _nvcc()
@@ -71,6 +80,7 @@ def build(verbose: bool = False, force: bool = False) -> str:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)
     build_driver(verbose=verbose, force=True)
+    build_pseudospectral(verbose=verbose, force=True)
     return LIB
 
 
@@ -86,6 +96,29 @@ def build_driver(verbose: bool = False, force: bool = False) -> str:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)
     return DRIVER
+
+
+def build_pseudospectral(verbose: bool = False, force: bool = False) -> str:
+    """libpseudospectral.so (FlatChannelSolver of the reference's solver layer
+    over the plugin classes) and, when the reference's main/channelflat.cc is
+    at hand, that main program linked against it unchanged."""
+    hdrs = [os.path.join(INCLUDE, h) for h in ("turbid_plugin.hpp", "turbid_gpu.h", "system.h",
+                                               "solver_channel_flat.h")]
+    cxx = shutil.which("g++") or "c++"
+    if force or not _newer(PSLIB, [PSLIB_SRC, LIB] + hdrs):
+        cmd = [cxx, "-O2", "-std=c++17", "-Wall", "-fPIC", "-shared", "-I", INCLUDE, PSLIB_SRC, "-L", HERE,
+               "-lturbid_gpu", "-Wl,-rpath,$ORIGIN", "-o", PSLIB]
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.run(cmd, check=True)
+    main_src = os.path.join(REFERENCE, "main", "channelflat.cc")
+    if os.path.isfile(main_src) and (force or not _newer(REF_MAIN, [main_src, PSLIB] + hdrs)):
+        cmd = [cxx, "-O2", "-std=c++17", "-I", INCLUDE, main_src, "-L", HERE, "-lpseudospectral",
+               "-Wl,-rpath,$ORIGIN", "-o", REF_MAIN]
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.run(cmd, check=True)
+    return PSLIB
 
 
 if __name__ == "__main__":

@@ -98,6 +98,10 @@ struct Ctx {
   double *gz = nullptr, *glz = nullptr, *d1r0 = nullptr, *d1rn = nullptr;
   int* yidx = nullptr;
   ZOperator opD1, opD2, opTmp, opEinv[5], opE[5];
+  // z-solver of the dense Helmholtz solves in mixed precision: FP64 DMMA
+  // (TG_ZSOLVER_DMMA) or the int8-slice tensor-core product (TG_ZSOLVER_ISLICE)
+  int zsolver = TG_ZSOLVER_DMMA;
+  IsliceOp* islTmp = nullptr;
   double* lamd[5] = {nullptr};
   FftPlan px, py;
   TransformDims td{};
@@ -177,6 +181,11 @@ struct Ctx {
     }
   }
   ~Ctx() {
+    for (int i = 0; i < 5; ++i) {
+      islice_destroy(opEinv[i].isl);
+      islice_destroy(opE[i].isl);
+    }
+    islice_destroy(islTmp);
     drop_graphs();
     release_overlap();
     if (cap_s) cudaStreamDestroy(cap_s);
@@ -213,7 +222,15 @@ static void install_decomposition(Ctx& x, int which) {
     fold_decomposition(x.dec[which], which == 3, Ei, E);
     zop_build(x.opEinv[which], Ei, x.nz, false, allocator(x));
     zop_build(x.opE[which], E, x.nz, false, allocator(x));
+    // the int8-slice form of the two products (mixed precision, interior of
+    // at most 256 rows); used while the z-solver selects it
+    if (x.mixed && x.nz - 2 <= 256) {
+      auto bytes = [&x](size_t n) -> void* { return x.dalloc<unsigned char>(n); };
+      islice_build(x.opEinv[which].isl, Ei, x.nz, x.nz, 5, x.M, bytes);
+      islice_build(x.opE[which].isl, E, x.nz, x.nz, 5, x.M, bytes);
+    }
   }
+  x.opEinv[which].use_isl = x.opE[which].use_isl = x.zsolver == TG_ZSOLVER_ISLICE;
   if (!x.lamd[which]) x.lamd[which] = x.dalloc<double>(x.nz);
   TG_CUDA(cudaMemcpy(x.lamd[which], x.dec[which].lam.data(), sizeof(double) * x.nz, cudaMemcpyHostToDevice));
 }
@@ -1734,6 +1751,34 @@ tg_status tg_dft_forward_f32(tg_ctx* ctx, const float* phys, double* spec, int d
   }
   TG_TRY(fwd<float>(x, phys, reinterpret_cast<double2*>(spec), dim * x.nz));
 }
+tg_status tg_dft_forward_planes(tg_ctx* ctx, const void* phys, double* spec, int planes, int fp32) {
+  TG_CHECK_CTX(ctx);
+  Ctx& x = *reinterpret_cast<Ctx*>(ctx);
+  if (!phys || !spec || planes < 1) {
+    set_error("RealCplxCube::DftForward > bad argument");
+    return TG_ERR_ARG;
+  }
+  TG_TRY({
+    if (fp32)
+      fwd<float>(x, phys, reinterpret_cast<double2*>(spec), planes);
+    else
+      fwd<double>(x, phys, reinterpret_cast<double2*>(spec), planes);
+  });
+}
+tg_status tg_dft_backward_planes(tg_ctx* ctx, const double* spec, void* phys, int planes, int fp32) {
+  TG_CHECK_CTX(ctx);
+  Ctx& x = *reinterpret_cast<Ctx*>(ctx);
+  if (!phys || !spec || planes < 1) {
+    set_error("RealCplxCube::DftBackward > bad argument");
+    return TG_ERR_ARG;
+  }
+  TG_TRY({
+    if (fp32)
+      bwd<float>(x, reinterpret_cast<const double2*>(spec), phys, planes);
+    else
+      bwd<double>(x, reinterpret_cast<const double2*>(spec), phys, planes);
+  });
+}
 tg_status tg_dft_backward_f64(tg_ctx* ctx, const double* spec, double* phys, int dim) {
   TG_CHECK_CTX(ctx);
   Ctx& x = *reinterpret_cast<Ctx*>(ctx);
@@ -1770,6 +1815,70 @@ tg_status tg_multiply(tg_ctx* ctx, const double* A_host, const double* in, doubl
     zop_build(x.opTmp, A, x.nz, true, allocator(x));
     gemm(x, x.opTmp, reinterpret_cast<const double2*>(in), x.S, reinterpret_cast<double2*>(out), x.S, dim,
          EpiParams());
+  });
+}
+
+tg_status tg_multiply_islice(tg_ctx* ctx, const double* A_host, const double* in, double* out, int dim) {
+  TG_CHECK_CTX(ctx);
+  Ctx& x = *reinterpret_cast<Ctx*>(ctx);
+  if (!A_host || !in || !out || dim < 1) {
+    set_error("RealCplxCube::Multiply > bad argument");
+    return TG_ERR_ARG;
+  }
+  if (in == out) {
+    set_error("RealCplxCube::Multiply(cmat,RealCplxCube) > Can not Do In-place Multiplication!");
+    return TG_ERR_ARG;
+  }
+  if (x.nz - 2 > 256) {
+    set_error("RealCplxCube::Multiply > the int8-slice product needs nz <= 258");
+    return TG_ERR_SHAPE;
+  }
+  TG_TRY({
+    TG_CUDA(cudaStreamSynchronize(x.s));
+    std::vector<double> A(A_host, A_host + (size_t)x.nz * x.nz);
+    auto bytes = [&x](size_t n) -> void* { return x.dalloc<unsigned char>(n); };
+    islice_build(x.islTmp, A, x.nz, x.nz, 5, x.M, bytes);
+    EpiParams ep;
+    ep.nz = x.nz;
+    ep.M = x.M;
+    islice_apply(*x.islTmp, reinterpret_cast<const double2*>(in), x.S, reinterpret_cast<double2*>(out), x.S, x.M,
+                 dim, ep, x.s);
+    TG_CUDA(cudaStreamSynchronize(x.s));
+    if (islice_error(*x.islTmp)) throw Error{TG_ERR_TIMEOUT, "RealCplxCube::Multiply > a bounded device wait gave up"};
+  });
+}
+
+tg_status tg_set_zsolver(tg_ctx* ctx, int solver) {
+  TG_CHECK_CTX(ctx);
+  Ctx& x = *reinterpret_cast<Ctx*>(ctx);
+  if (solver != TG_ZSOLVER_DMMA && solver != TG_ZSOLVER_ISLICE) {
+    set_error("tg_set_zsolver > unknown z-solver");
+    return TG_ERR_ARG;
+  }
+  TG_TRY({
+    TG_CUDA(cudaStreamSynchronize(x.s));
+    x.zsolver = solver;
+    for (int i = 0; i < 5; ++i)
+      x.opEinv[i].use_isl = x.opE[i].use_isl = solver == TG_ZSOLVER_ISLICE && x.opEinv[i].isl && x.opE[i].isl;
+    x.drop_graphs();
+  });
+}
+
+tg_status tg_zsolver_error(tg_ctx* ctx, int* flag) {
+  TG_CHECK_CTX(ctx);
+  Ctx& x = *reinterpret_cast<Ctx*>(ctx);
+  if (!flag) {
+    set_error("tg_zsolver_error > null argument");
+    return TG_ERR_ARG;
+  }
+  TG_TRY({
+    TG_CUDA(cudaStreamSynchronize(x.s));
+    int f = 0;
+    for (int i = 0; i < 5; ++i) {
+      if (x.opEinv[i].isl) f |= islice_error(*x.opEinv[i].isl);
+      if (x.opE[i].isl) f |= islice_error(*x.opE[i].isl);
+    }
+    *flag = f;
   });
 }
 

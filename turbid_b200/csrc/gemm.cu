@@ -553,15 +553,38 @@ static void zgemm_launch(const ZProblem* probs, int nprob, int M, cudaStream_t s
 
 // Problems of one kernel shape share a launch; a group that mixes dense,
 // folded and split-input operators runs as one launch per shape.
+// Dense operators with an int8-slice form (use_isl) take the tensor-core
+// slice product for single-component problems with a STORE or RSCALE
+// epilogue, grouped when their operators differ (each owns its scratch).
 void zgemm_group(const ZProblem* probs, int nprob, int M, cudaStream_t s) {
   if (nprob < 1 || nprob > kMaxGroup) throw Error{TG_ERR_ARG, "zgemm > bad group size"};
   ZProblem part[3][kMaxGroup];
   int np[3] = {0, 0, 0};
+  const IsliceOp* iops[kMaxGroup];
+  const double2* iins[kMaxGroup];
+  double2* iouts[kMaxGroup];
+  EpiParams ieps[kMaxGroup];
+  int ni = 0;
   for (int i = 0; i < nprob; ++i) {
     const ZOperator& op = *probs[i].op;
+    const bool isl = op.isl && op.use_isl && !op.sym && probs[i].batch == 1 &&
+                     (probs[i].ep.mode == EPI_STORE || probs[i].ep.mode == EPI_RSCALE);
+    bool shared_op = false;
+    for (int k = 0; k < ni; ++k) shared_op |= iops[k] == op.isl;
+    if (isl && !shared_op) {
+      iops[ni] = op.isl;
+      iins[ni] = probs[i].in;
+      iouts[ni] = probs[i].out;
+      ieps[ni] = probs[i].ep;
+      ieps[ni].nz = op.n;
+      ieps[ni].M = M;
+      ++ni;
+      continue;
+    }
     const int k = !op.sym ? 0 : (op.split == 2 ? 2 : 1);
     part[k][np[k]++] = probs[i];
   }
+  if (ni) islice_group(iops, iins, iouts, ieps, ni, M, s);
   for (int k = 0; k < 3; ++k)
     if (np[k]) zgemm_launch(part[k], np[k], M, s);
 }
@@ -649,6 +672,13 @@ static void zgemm_launch(const ZProblem* probs, int nprob, int M, cudaStream_t s
 
 void zgemm(const ZOperator& op, const double2* in, long long in_stride, double2* out, long long out_stride, int M,
            int batch, const EpiParams& ep, cudaStream_t s) {
+  if (op.isl && op.use_isl && !op.sym && batch > 1 && (ep.mode == EPI_STORE || ep.mode == EPI_RSCALE)) {
+    EpiParams e = ep;
+    e.nz = op.n;
+    e.M = M;
+    islice_apply(*op.isl, in, in_stride, out, out_stride, M, batch, e, s);
+    return;
+  }
   ZProblem p{&op, in, in_stride, out, out_stride, batch, ep};
   zgemm_group(&p, 1, M, s);
 }

@@ -1,0 +1,545 @@
+// FP64-accurate z-operator products from exact int8 tensor-core products
+// (tcgen05.mma kind::i8, accumulators in tensor memory), for the dense
+// Helmholtz solves of the mixed precision mode
+// (reference: the E^-1 / E products of FlatCarrierPhase::Helmholtz and
+// FlatScalarPhase::Helmholtz, src/phase_carrier_flat.cc:861-994,
+// src/phase_scalar_flat.cc:635-667, through RealCplxCube::Multiply,
+// src/cube_real_cplx.cc:461-471).
+//
+// Splitting (Ozaki, Ogita, Oishi, Rump, "Error-free transformations of matrix
+// multiplication", Numer. Algorithms 2012; integer slices as in Ootomo, Ozaki,
+// Yokota, "DGEMM on integer matrix multiplication unit", 2024):
+//   * the operator by rows and the data by columns, over the interior rows
+//     k = 1 .. nz-2 only, into S slices of integers of magnitude <= 64, each
+//     row / column scaled by a power of two 2^e with e from frexp of its
+//     largest magnitude (|x| 2^-e <= 1): slice 0 = rint(64 r), slice p > 0 =
+//     rint(128 r') of the remainder r' -- every step exact in FP64;
+//   * the slice pairs (p, q) with p + q < S multiplied exactly in int32, one
+//     tensor-memory accumulator per diagonal d = p + q;
+//   * the diagonals combined in FP64 with weight 2^-(12+7d), d ascending (one
+//     fma each, exact product), then the row and column scales;
+//   * the two boundary rows of the data (z = 0 and z = nz-1; the scalar's
+//     Robin rows carry values scaled by 1e7) as an FP64 rank-2 update:
+//     out = (A[r][0] x0 + interior) + A[r][nz-1] x_{nz-1}.
+//
+// Layouts: one K-major tile per 128 data columns and slice (the MMA's A
+// operand, M = 128 columns, K = 256 interior rows padded with zeros) and one
+// K-major tile per BN operator rows and slice (the B operand, N = BN), both
+// written in the canonical no-swizzle core-matrix order (8 rows x 16 bytes,
+// K chunks 128 bytes apart, 8-row groups 2048 bytes apart) so that each tile
+// is one contiguous bulk copy into shared memory.  The CTA keeps its 128
+// columns' S data tiles in shared memory, walks the operator in chunks of BN
+// rows (double-buffered bulk copies), and one thread issues the MMAs; after
+// each chunk every thread reads its column's S accumulators from tensor memory
+// (thread i = lane i = data column c0 + i) and stores the chunk's rows of its
+// column, coalesced across the warp.  Every wait is bounded: a wait that gives
+// up sets the error flag, the kernel drains what it issued (bounded too),
+// frees its tensor memory and returns.
+#include <cfloat>
+#include <climits>
+#include <cstdint>
+#include <memory>
+#include <vector>
+
+#include "tg_common.cuh"
+
+namespace tg {
+namespace {
+
+constexpr int KP = 256;                 // interior rows padded to 8 MMA K-steps of 32
+constexpr int BM = 128;                 // data columns per CTA (MMA M, tensor-memory lanes)
+constexpr int kThreads = 128;
+constexpr int kTileX = BM * KP;         // bytes of one data tile
+constexpr int kBadExp = INT_MIN;        // column exponent of a column holding NaN or inf
+constexpr long long kSpin = 1ll << 22;  // polls of a bounded wait (each try_wait may suspend)
+
+template <int S>
+struct IslShape {
+  static constexpr int BN = S <= 5 ? 96 : (S == 6 ? 80 : 64);   // S * BN accumulator columns <= 512
+  static constexpr int kTileA = BN * KP;
+  static constexpr size_t kSmem = (size_t)S * kTileX + 2 * (size_t)kTileA;
+  static_assert(S * BN <= 512, "one accumulator per slice diagonal must fit tensor memory");
+  static_assert(BN % 16 == 0 && BN >= 16 && BN <= 256, "MMA N for M = 128");
+};
+
+__host__ __device__ constexpr int kmaj_off(int row, int k) {
+  return (row >> 3) * (KP / 16) * 128 + (k >> 4) * 128 + (row & 7) * 16 + (k & 15);
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// shared-memory matrix descriptor: canonical K-major layout, no swizzle
+__device__ __forceinline__ uint64_t smem_desc(uint32_t saddr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFF);                        // start address
+  d |= (uint64_t)((128 >> 4) & 0x3FFF) << 16;                    // leading byte offset: K chunks
+  d |= (uint64_t)((((KP / 16) * 128) >> 4) & 0x3FFF) << 32;      // stride byte offset: 8-row groups
+  d |= (uint64_t)1 << 46;                                        // descriptor version (sm_100)
+  return d;                                                      // base offset 0, no swizzle
+}
+
+// instruction descriptor: s32 accumulator, signed 8-bit A and B, both K-major
+__host__ __device__ constexpr uint32_t idesc_i8(int M, int N) {
+  return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+// true once the phase with the given parity has completed; false after kSpin polls
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+  for (long long i = 0; i < kSpin; ++i) {
+    uint32_t done = 0;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+// global -> shared bulk copy (16-byte aligned, size a multiple of 16), completion on bar
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(bar)
+               : "memory");
+}
+
+__device__ __forceinline__ double max_keep_nan(double a, double b) { return (b > a || isnan(b)) ? b : a; }
+
+// ---------------------------------------------------------------------------
+// Data slicing: four threads per column of a 128-column tile (512 threads).
+// Each finds the maximum magnitude over a quarter of the interior rows; the
+// column's exponent follows from their maximum; then each writes the S slices
+// of a quarter of the K range in the tile image order (16 K values = one
+// 16-byte chunk at a time).  blockIdx.y selects the problem of a group.
+// ---------------------------------------------------------------------------
+constexpr int kMaxIsl = 3;
+constexpr int kSliceThreads = 4 * BM;
+
+struct SliceArgs {
+  const double* in[kMaxIsl];   // FP64 component, row-major [nz][ncol]
+  int8_t* xs[kMaxIsl];         // data tiles [tile][S][kTileX]
+  int* xe[kMaxIsl];            // column exponents [tile * 128 + i]
+  int nz, ncol, ntiles;
+};
+
+template <int S>
+__global__ void __launch_bounds__(kSliceThreads) k_slice_data(const SliceArgs a) {
+  __shared__ double part_max[4][BM];
+  const int t = threadIdx.x & (BM - 1), part = threadIdx.x >> 7;
+  const int tile = blockIdx.x, pb = blockIdx.y;
+  const int c = tile * BM + t;
+  const bool valid = c < a.ncol;
+  const double* X = a.in[pb];
+  const int nin = a.nz - 2;                       // interior rows z = 1 .. nz-2
+  const int z0 = 1 + part * ((nin + 3) / 4), z1 = min(a.nz - 1, z0 + (nin + 3) / 4);
+  double mx = 0.0;
+  if (valid)
+    for (int z = z0; z < z1; ++z) mx = max_keep_nan(mx, fabs(X[(size_t)z * a.ncol + c]));
+  part_max[part][t] = mx;
+  __syncthreads();
+  mx = max_keep_nan(max_keep_nan(part_max[0][t], part_max[1][t]), max_keep_nan(part_max[2][t], part_max[3][t]));
+  int e = 0;
+  const bool bad = !(mx <= DBL_MAX);
+  if (!bad && mx > 0.0) {
+    int ee = 0;
+    const double f = frexp(mx, &ee);
+    e = f == 0.5 ? ee - 1 : ee;
+  }
+  if (valid && part == 0) a.xe[pb][tile * BM + t] = bad ? kBadExp : e;
+  int8_t* dst = a.xs[pb] + (size_t)tile * S * kTileX;
+  for (int kc = part * 4; kc < part * 4 + 4; ++kc) {
+    uint32_t w[S][4];
+#pragma unroll
+    for (int p = 0; p < S; ++p)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) w[p][j] = 0u;
+#pragma unroll
+    for (int kk = 0; kk < 16; ++kk) {
+      const int z = kc * 16 + kk + 1;
+      const double x = (valid && !bad && z < a.nz - 1) ? X[(size_t)z * a.ncol + c] : 0.0;
+      double r = ldexp(x, -e);
+      double q = rint(r * 64.0);
+      r = r * 64.0 - q;
+      w[0][kk >> 2] |= ((uint32_t)(__double2int_rn(q) & 0xff)) << (8 * (kk & 3));
+#pragma unroll
+      for (int p = 1; p < S; ++p) {
+        q = rint(r * 128.0);
+        r = r * 128.0 - q;
+        w[p][kk >> 2] |= ((uint32_t)(__double2int_rn(q) & 0xff)) << (8 * (kk & 3));
+      }
+    }
+#pragma unroll
+    for (int p = 0; p < S; ++p)
+      *reinterpret_cast<uint4*>(dst + (size_t)p * kTileX + kmaj_off(t, kc * 16)) =
+          make_uint4(w[p][0], w[p][1], w[p][2], w[p][3]);
+  }
+}
+
+struct IslProblem {
+  const int8_t* xs;     // data tiles [tile][S][kTileX]
+  const int* xe;        // column exponents [tile * 128 + i]
+  const int8_t* as;     // operator chunk tiles [chunk][S][BN * KP]
+  const double* a0;     // [rows_pad] A[r][0]
+  const double* an;     // [rows_pad] A[r][nz-1]
+  const double* asc;    // [rows_pad] 2^(row exponent)
+  const double* in;     // FP64 input component (its boundary rows are read)
+  double* out;
+  EpiParams ep;         // EPI_STORE or EPI_RSCALE
+};
+struct IslArgs {
+  IslProblem p[kMaxIsl];   // blockIdx.y selects the problem
+  int nz, nrow, ncol, ntiles, nchunks;
+  int* err;
+};
+
+template <int S>
+__global__ void __launch_bounds__(kThreads, 1) k_islice_gemm(const IslArgs args) {
+  using Sh = IslShape<S>;
+  constexpr int BN = Sh::BN;
+  constexpr uint32_t idesc = idesc_i8(BM, BN);
+  extern __shared__ __align__(1024) uint8_t sm[];
+  uint8_t* sx = sm;                                   // S data tiles
+  uint8_t* sa = sm + (size_t)S * kTileX;              // two operator tiles
+  __shared__ __align__(8) uint64_t bars[6];           // 0 data, 1-2 full, 3-4 empty, 5 accumulators
+  __shared__ uint32_t tmem_slot;
+  __shared__ int s_err;
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const int tile = blockIdx.x;
+  const IslProblem& a = args.p[blockIdx.y];
+  const uint32_t bar_x = smem_u32(&bars[0]), bar_acc = smem_u32(&bars[5]);
+  auto bar_full = [&](int i) { return smem_u32(&bars[1 + i]); };
+  auto bar_empty = [&](int i) { return smem_u32(&bars[3 + i]); };
+  const int total = args.nchunks * S;   // (chunk, operator slice) iterations
+
+  if (tid == 0) {
+    s_err = 0;
+    for (int i = 0; i < 6; ++i) mbar_init(smem_u32(&bars[i]), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(smem_u32(&tmem_slot)));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  const uint32_t tmem = tmem_slot;
+
+  // bulk loads issued per operator buffer, so that an early exit can drain them
+  int nload[2] = {0, 0};
+  auto issue_op_load = [&](int it) {
+    const int buf = it & 1;
+    const int8_t* src = a.as + (size_t)it * Sh::kTileA;   // chunk-major, slice-minor = iteration order
+    mbar_expect_tx(bar_full(buf), Sh::kTileA);
+    bulk_g2s(smem_u32(sa + buf * Sh::kTileA), src, Sh::kTileA, bar_full(buf));
+    ++nload[buf];
+  };
+  if (tid == 0) {
+    mbar_expect_tx(bar_x, S * kTileX);
+    for (int p = 0; p < S; ++p)
+      bulk_g2s(smem_u32(sx + p * kTileX), a.xs + ((size_t)tile * S + p) * kTileX, kTileX, bar_x);
+    issue_op_load(0);
+    if (total > 1) issue_op_load(1);
+    if (!mbar_wait(bar_x, 0)) s_err = 1;
+  }
+
+  // per-thread column constants
+  const int ncol = args.ncol, nz = args.nz;
+  const int c = tile * BM + tid;
+  const bool valid = c < ncol;
+  const double xb = valid ? a.in[c] : 0.0;
+  const double xt = valid ? a.in[(size_t)(nz - 1) * ncol + c] : 0.0;
+  const int e = valid ? a.xe[tile * BM + tid] : 0;
+  const bool bad = e == kBadExp;
+  const double csc = bad ? 0.0 : ldexp(1.0, e);
+  const int m = c >> 1;
+  const bool rscale = a.ep.mode == EPI_RSCALE;
+  const double k2m = (rscale && valid) ? a.ep.k2[m] : 0.0;
+  double* out = a.out;
+
+  int it = 0;
+  for (int j = 0; j < args.nchunks; ++j) {
+    if (tid == 0 && !s_err) {
+      for (int p = 0; p < S; ++p, ++it) {
+        const int buf = it & 1;
+        if (!mbar_wait(bar_full(buf), (it >> 1) & 1)) {
+          s_err = 1;
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        const uint32_t sa_addr = smem_u32(sa + buf * Sh::kTileA);
+        for (int q = 0; q < S - p; ++q) {
+          const uint32_t dacc = tmem + (uint32_t)((p + q) * BN);
+          const uint32_t sx_addr = smem_u32(sx + q * kTileX);
+#pragma unroll
+          for (int kk = 0; kk < KP / 32; ++kk) {
+            const uint64_t da = smem_desc(sx_addr + kk * 256);
+            const uint64_t db = smem_desc(sa_addr + kk * 256);
+            const uint32_t acc = (p == 0 && kk == 0) ? 0u : 1u;   // p = 0 opens every diagonal
+            asm volatile(
+                "{\n\t.reg .pred pd;\n\t"
+                "setp.ne.b32 pd, %4, 0;\n\t"
+                "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, pd;\n\t}" ::"r"(dacc),
+                "l"(da), "l"(db), "r"(idesc), "r"(acc));
+          }
+        }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+            bar_empty(buf)));
+        // refill the other buffer for the next iteration once the MMAs that read it are done
+        const int next = it + 1;
+        if (next >= 2 && next < total) {
+          if (!mbar_wait(bar_empty(next & 1), ((next - 2) >> 1) & 1)) {
+            s_err = 1;
+            ++it;
+            break;
+          }
+          issue_op_load(next);
+        }
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar_acc));
+    }
+    // every thread: the chunk's accumulators are complete
+    bool ok = mbar_wait(bar_acc, j & 1);
+    ok = __all_sync(0xffffffffu, ok);   // warp-uniform: the tensor-memory loads below are .sync.aligned
+    if (!ok) s_err = 1;
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    if (ok) {
+      const int r0 = j * BN;
+#pragma unroll 1
+      for (int jg = 0; jg < BN; jg += 16) {
+        double acc[16];
+#pragma unroll
+        for (int i = 0; i < 16; ++i) acc[i] = 0.0;
+#pragma unroll 1
+        for (int d = 0; d < S; ++d) {
+          uint32_t v[16];
+          const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(d * BN + jg);
+          asm volatile(
+              "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
+              "[%16];"
+              : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+                "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
+                "=r"(v[15])
+              : "r"(taddr));
+          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+          const double w = ldexp(1.0, -(12 + 7 * d));
+#pragma unroll
+          for (int i = 0; i < 16; ++i) acc[i] = __fma_rn((double)(int)v[i], w, acc[i]);
+        }
+        if (valid) {
+#pragma unroll
+          for (int i = 0; i < 16; ++i) {
+            const int r = r0 + jg + i;
+            if (r < args.nrow) {
+              const double interior = __dmul_rn(__dmul_rn(acc[i], __ldg(a.asc + r)), csc);
+              double v = __dadd_rn(__dadd_rn(__dmul_rn(__ldg(a.a0 + r), xb), interior), __dmul_rn(__ldg(a.an + r), xt));
+              if (bad) v = __longlong_as_double(0x7ff8000000000000LL);
+              if (rscale && r != 0 && r != nz - 1) {
+                const double lam = __ldg(a.ep.lam + r);
+                double R = 1.0 / ((k2m + lam) + a.ep.sigma);
+                if (a.ep.null_mode && m == 0 && fabs(lam) < 10e-12) R = 0.0;
+                v = __dmul_rn(v, R);
+              }
+              out[(size_t)r * ncol + c] = v;
+            }
+          }
+        }
+      }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();   // accumulators read before the next chunk's MMAs overwrite them
+    if (s_err) break;  // uniform: read after the barrier
+  }
+  // drain: every bulk copy issued must have landed before the shared memory is
+  // released (the MMAs were awaited through the accumulator barrier)
+  if (tid == 0 && s_err) {
+    mbar_wait(bar_x, 0);
+    for (int k = 0; k < 2; ++k)
+      if (nload[k] > 0) mbar_wait(bar_full(k), (nload[k] - 1) & 1);
+    atomicExch(args.err, 1);
+  }
+  __syncthreads();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tmem));
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+struct IsliceOp {
+  int S = 0, nz = 0, nrow = 0, nchunks = 0, BN = 0;
+  int8_t* as = nullptr;   // operator chunk tiles
+  double* aux = nullptr;  // a0, an, asc: 3 x rows_pad
+  // slicing scratch for one component of M modes
+  int8_t* xs = nullptr;
+  int* xe = nullptr;
+  int ntiles = 0, ncol = 0;
+  int* err = nullptr;
+};
+
+namespace {
+template <int S>
+void islice_set_smem() {
+  TG_CUDA(cudaFuncSetAttribute(k_islice_gemm<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)IslShape<S>::kSmem));
+}
+}  // namespace
+
+// Slices of an nrow x nz operator (row-major FP64) for S slices, in the chunk
+// tile order of the kernel; the same rule as the data slicing, per row over
+// the interior columns.  Returns the row exponents' scales and the boundary
+// columns in aux.
+static void slice_operator_host(const std::vector<double>& A, int nrow, int nz, int S, int BN, int nchunks,
+                                std::vector<int8_t>& tiles, std::vector<double>& aux) {
+  const int rows_pad = nchunks * BN;
+  tiles.assign((size_t)nchunks * S * BN * KP, 0);
+  aux.assign((size_t)3 * rows_pad, 0.0);
+  for (int r = 0; r < nrow; ++r) {
+    double mx = 0.0;
+    for (int k = 1; k < nz - 1; ++k) mx = std::max(mx, std::fabs(A[(size_t)r * nz + k]));
+    int e = 0;
+    if (mx > 0.0) {
+      int ee = 0;
+      const double f = std::frexp(mx, &ee);
+      e = f == 0.5 ? ee - 1 : ee;
+    }
+    aux[r] = A[(size_t)r * nz];
+    aux[rows_pad + r] = A[(size_t)r * nz + nz - 1];
+    aux[2 * rows_pad + r] = std::ldexp(1.0, e);
+    const int j = r / BN, rr = r % BN;
+    for (int k = 0; k + 1 < nz - 1; ++k) {
+      double x = std::ldexp(A[(size_t)r * nz + k + 1], -e);
+      double q = std::rint(x * 64.0);
+      x = x * 64.0 - q;
+      tiles[((size_t)j * S + 0) * BN * KP + kmaj_off(rr, k)] = (int8_t)(int)q;
+      for (int p = 1; p < S; ++p) {
+        q = std::rint(x * 128.0);
+        x = x * 128.0 - q;
+        tiles[((size_t)j * S + p) * BN * KP + kmaj_off(rr, k)] = (int8_t)(int)q;
+      }
+    }
+  }
+}
+
+void islice_build(IsliceOp*& op, const std::vector<double>& A, int nrow, int nz, int S, int M,
+                  const std::function<void*(size_t)>& alloc) {
+  if (S != 5) throw Error{TG_ERR_ARG, "islice > only 5 slices are built"};
+  if (nz < 3 || nz - 2 > KP) throw Error{TG_ERR_SHAPE, "islice > nz - 2 must be at most 256"};
+  if ((size_t)A.size() != (size_t)nrow * nz) throw Error{TG_ERR_SHAPE, "islice > operator size"};
+  static bool smem_set = false;
+  if (!smem_set) {
+    islice_set_smem<5>();
+    smem_set = true;
+  }
+  const int BN = IslShape<5>::BN, nchunks = (nrow + BN - 1) / BN;
+  if (op && (op->nz != nz || op->nrow != nrow || op->ncol != 2 * M))
+    throw Error{TG_ERR_SHAPE, "islice > rebuild with another shape"};
+  std::vector<int8_t> tiles;
+  std::vector<double> aux;
+  slice_operator_host(A, nrow, nz, S, BN, nchunks, tiles, aux);
+  if (!op) {
+    std::unique_ptr<IsliceOp> o(new IsliceOp);
+    o->S = S;
+    o->nz = nz;
+    o->nrow = nrow;
+    o->BN = BN;
+    o->nchunks = nchunks;
+    o->ncol = 2 * M;
+    o->ntiles = (o->ncol + BM - 1) / BM;
+    o->as = static_cast<int8_t*>(alloc(tiles.size()));
+    o->aux = static_cast<double*>(alloc(aux.size() * sizeof(double)));
+    o->xs = static_cast<int8_t*>(alloc((size_t)o->ntiles * S * kTileX));
+    o->xe = static_cast<int*>(alloc((size_t)o->ntiles * BM * sizeof(int)));
+    o->err = static_cast<int*>(alloc(sizeof(int)));
+    TG_CUDA(cudaMemset(o->err, 0, sizeof(int)));
+    op = o.release();
+  }
+  TG_CUDA(cudaMemcpy(op->as, tiles.data(), tiles.size(), cudaMemcpyHostToDevice));
+  TG_CUDA(cudaMemcpy(op->aux, aux.data(), aux.size() * sizeof(double), cudaMemcpyHostToDevice));
+}
+
+void islice_destroy(IsliceOp* op) { delete op; }   // device buffers belong to the allocator's owner
+
+// Problems of one group: each batch component of each problem is one problem of
+// the launch pair (slicing, then product), at most kMaxIsl per pair.
+void islice_group(const IsliceOp* const* ops, const double2* const* ins, double2* const* outs,
+                  const EpiParams* eps, int n, int M, cudaStream_t s) {
+  using Sh = IslShape<5>;
+  if (n < 1 || n > kMaxIsl) throw Error{TG_ERR_ARG, "islice > bad group size"};
+  const IsliceOp& op0 = *ops[0];
+  SliceArgs sa{};
+  IslArgs a{};
+  for (int i = 0; i < n; ++i) {
+    const IsliceOp& op = *ops[i];
+    if (2 * M != op.ncol || op.nz != op0.nz || op.nrow != op0.nrow)
+      throw Error{TG_ERR_SHAPE, "islice > operators of one group differ in shape"};
+    if (eps[i].mode != EPI_STORE && eps[i].mode != EPI_RSCALE)
+      throw Error{TG_ERR_ARG, "islice > unsupported epilogue"};
+    if (reinterpret_cast<const void*>(ins[i]) == reinterpret_cast<const void*>(outs[i]))
+      throw Error{TG_ERR_ARG, "islice > input and output must differ"};
+    sa.in[i] = reinterpret_cast<const double*>(ins[i]);
+    sa.xs[i] = op.xs;
+    sa.xe[i] = op.xe;
+    IslProblem& p = a.p[i];
+    const int rows_pad = op.nchunks * op.BN;
+    p.xs = op.xs;
+    p.xe = op.xe;
+    p.as = op.as;
+    p.a0 = op.aux;
+    p.an = op.aux + rows_pad;
+    p.asc = op.aux + 2 * rows_pad;
+    p.in = reinterpret_cast<const double*>(ins[i]);
+    p.out = reinterpret_cast<double*>(outs[i]);
+    p.ep = eps[i];
+  }
+  sa.nz = op0.nz;
+  sa.ncol = op0.ncol;
+  sa.ntiles = op0.ntiles;
+  a.nz = op0.nz;
+  a.nrow = op0.nrow;
+  a.ncol = op0.ncol;
+  a.ntiles = op0.ntiles;
+  a.nchunks = op0.nchunks;
+  a.err = op0.err;
+  const double by = n * (16.0 * M * op0.nz * 2 + (double)op0.ntiles * 5 * kTileX * 2);
+  const double fl = n * 4.0 * op0.nz * op0.nz * (double)M;
+  prof_begin(s, PC_GEMM, by, fl, fl);
+  k_slice_data<5><<<dim3(op0.ntiles, n), kSliceThreads, 0, s>>>(sa);
+  TG_LAUNCH_CHECK("k_slice_data");
+  k_islice_gemm<5><<<dim3(op0.ntiles, n), kThreads, Sh::kSmem, s>>>(a);
+  prof_end(s);
+  TG_LAUNCH_CHECK("k_islice_gemm");
+}
+
+// out = epi(A in) for `batch` components of M modes (strides in complex
+// elements), in groups through the op's single slicing scratch: the
+// components run one after another.
+void islice_apply(const IsliceOp& op, const double2* in, long long in_stride, double2* out, long long out_stride,
+                  int M, int batch, const EpiParams& ep, cudaStream_t s) {
+  for (int b = 0; b < batch; ++b) {
+    const IsliceOp* o = &op;
+    const double2* i = in + (size_t)b * in_stride;
+    double2* r = out + (size_t)b * out_stride;
+    islice_group(&o, &i, &r, &ep, 1, M, s);
+  }
+}
+
+// The error flag of the op's bounded waits (a synchronous read: call between steps).
+int islice_error(const IsliceOp& op) {
+  int v = 0;
+  TG_CUDA(cudaMemcpy(&v, op.err, sizeof(int), cudaMemcpyDeviceToHost));
+  return v;
+}
+
+}  // namespace tg

@@ -196,6 +196,23 @@ struct EpiParams {
   long long sX = 0, sH = 0, sU = 0, sAux = 0;
 };
 
+// FP64-accurate product from exact int8 tensor-core slices (islice.cu): the
+// operator's slices and the data-slicing scratch of one component.
+struct IsliceOp;
+// Slices of the nrow x nz row-major operator A (S = 5), for products over
+// components of M modes; op is built on the first call and refilled (same
+// shape) on later ones.  Device memory through alloc (owned by the caller).
+void islice_build(IsliceOp*& op, const std::vector<double>& A, int nrow, int nz, int S, int M,
+                  const std::function<void*(size_t)>& alloc);
+void islice_destroy(IsliceOp* op);
+// n <= 3 problems (distinct operators), one launch pair: out_i = epi_i(A_i in_i)
+void islice_group(const IsliceOp* const* ops, const double2* const* ins, double2* const* outs,
+                  const EpiParams* eps, int n, int M, cudaStream_t s);
+void islice_apply(const IsliceOp& op, const double2* in, long long in_stride, double2* out, long long out_stride,
+                  int M, int batch, const EpiParams& ep, cudaStream_t s);
+// the error flag of the product's bounded waits (synchronous read)
+int islice_error(const IsliceOp& op);
+
 // A real nz x nz operator resident on the device: the dense copy and, when
 // it is centro-symmetric (sgn +1) or centro-antisymmetric (sgn -1), the two
 // folded halves used by the half-flop kernel.
@@ -217,6 +234,10 @@ struct ZOperator {
   double* A = nullptr;
   double* Ae = nullptr;
   double* Ao = nullptr;
+  // int8-slice form of a dense operator (mixed precision solves); used by
+  // zgemm for the STORE and RSCALE epilogues when use_isl is set
+  IsliceOp* isl = nullptr;
+  bool use_isl = false;
 };
 
 // One problem of a grouped launch: batch components of `in` (stride in_stride

@@ -125,6 +125,12 @@ class ChannelCase:
         """Replay whole RK3 steps of run_steps as CUDA graphs (default) or not."""
         check(self.lib.tg_set_graphs(self.h, int(bool(enable))))
 
+    def set_zsolver(self, solver: str):
+        """Products of the dense Helmholtz solves in mixed precision: "dmma"
+        (FP64 tensor cores) or "islice" (exact int8 slices on the tcgen05
+        tensor cores)."""
+        check(self.lib.tg_set_zsolver(self.h, {"dmma": 0, "islice": 1}[solver]))
+
     def autotune(self, cache_path: Optional[str] = None) -> dict:
         """Pick the z-operator GEMM row tiling for this grid and GPU (timed, or
         read from the JSON cache at cache_path) and apply it; returns the
@@ -168,6 +174,16 @@ class ChannelCase:
     def dft_backward(self, spec_ptr: int, phys_ptr: int, dim: int, fp32: bool = False):
         fn = self.lib.tg_dft_backward_f32 if fp32 else self.lib.tg_dft_backward_f64
         check(fn(self.h, ctypes.c_void_p(spec_ptr), ctypes.c_void_p(phys_ptr), int(dim)))
+
+    def dft_forward_planes(self, phys_ptr: int, spec_ptr: int, planes: int, fp32: bool = False):
+        """Forward x/y transforms of `planes` physical z planes (a z-slab)."""
+        check(self.lib.tg_dft_forward_planes(self.h, ctypes.c_void_p(phys_ptr), ctypes.c_void_p(spec_ptr),
+                                             int(planes), int(bool(fp32))))
+
+    def dft_backward_planes(self, spec_ptr: int, phys_ptr: int, planes: int, fp32: bool = False):
+        """Backward y/x transforms of `planes` spectral z planes (a z-slab)."""
+        check(self.lib.tg_dft_backward_planes(self.h, ctypes.c_void_p(spec_ptr), ctypes.c_void_p(phys_ptr),
+                                              int(planes), int(bool(fp32))))
 
     def multiply(self, A: np.ndarray, in_ptr: int, out_ptr: int, dim: int):
         A = np.ascontiguousarray(A, dtype=np.float64)
