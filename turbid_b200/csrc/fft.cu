@@ -718,13 +718,15 @@ __global__ void __launch_bounds__(NB * L / 16) bx_p2_kernel(TransformDims d, con
 //   out_c = (u + su) d_c/dx + (v + sv) d_c/dy + (w + sw) d_c/dz
 // of the advective nonlinear form (phase_carrier_flat.cc:786-797,
 // phase_scalar_flat.cc:588-591), so the nine physical gradient fields are
-// never written.  grid: (row blocks, nz, ncomp); unl: the physical velocity.
+// never written.  grid: (row blocks x ncomp, nz) with the component fastest:
+// the ncomp CTAs of one row block run together, so the velocity rows they
+// share come from DRAM once and from L2 after; unl: the physical velocity.
 // FP32: registers capped for about 640 threads per SM (measured best).
 template <typename T, int L, int NB>
 __global__ void __launch_bounds__(NB * L / 16, sizeof(T) == 4 ? 640 / (NB * L / 16) : 1) bx_adv_p2_kernel(TransformDims d, const cplx<T>* __restrict__ tw,
                                                                const cplx<T>* __restrict__ work,
                                                                const T* __restrict__ unl, T* __restrict__ out,
-                                                               size_t P, double su, double sv, double sw) {
+                                                               size_t P, int ncomp, double su, double sv, double sw) {
   using C = cplx<T>;
   using PV = P2Vec<T>;
   using R = typename PV::R;
@@ -732,8 +734,8 @@ __global__ void __launch_bounds__(NB * L / 16, sizeof(T) == 4 ? 640 / (NB * L / 
   constexpr int IS = NB * L / (NT * VW);
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* buf = reinterpret_cast<C*>(smem_raw);
-  const int z = blockIdx.y, c = blockIdx.z;
-  const int y0 = blockIdx.x * rows;
+  const int z = blockIdx.y, c = blockIdx.x % ncomp;
+  const int y0 = (blockIdx.x / ncomp) * rows;
   const size_t zoff = (size_t)z * d.ny * L;
   R acca[IS], accb[IS];
 #pragma unroll
@@ -1028,13 +1030,16 @@ void dft_backward_adv(const TransformDims& d, const FftPlan& px, const FftPlan& 
   }
   {  // x pass and the advection sums
     const size_t P = (size_t)d.nx * d.ny * d.nz;
-    prof_begin(s, PC_FFT_BX, (double)ncomp * d.nz * d.ny * (3.0 * d.nxh * sizeof(C) + 4.0 * d.nx * sizeof(T)), 0);
+    // per component: three gradient intermediates in, one field out; the velocity once
+    prof_begin(s, PC_FFT_BX,
+               (double)d.nz * d.ny * (ncomp * (3.0 * d.nxh * sizeof(C) + 1.0 * d.nx * sizeof(T)) + 3.0 * d.nx * sizeof(T)),
+               0);
     const C* tw = Tw<T>::get(px);
 #define TG_CALL(LL)                                                                                  \
   {                                                                                                  \
     constexpr int NB = P2Elems<T, P2_BX>::value / LL;                                                \
-    dim3 grid((d.ny + 2 * NB - 1) / (2 * NB), d.nz, ncomp);                                          \
-    bx_adv_p2_kernel<T, LL, NB><<<grid, NB * LL / 16, p2_smem<T, LL, P2_BX>(), s>>>(d, tw, w, unl, out, P, su, sv, sw); \
+    dim3 grid((d.ny + 2 * NB - 1) / (2 * NB) * ncomp, d.nz);                                         \
+    bx_adv_p2_kernel<T, LL, NB><<<grid, NB * LL / 16, p2_smem<T, LL, P2_BX>(), s>>>(d, tw, w, unl, out, P, ncomp, su, sv, sw); \
   }
     TG_P2_DISPATCH(px.L, TG_CALL)
 #undef TG_CALL
