@@ -50,7 +50,7 @@ def _limit_after_first_step(cfg, uvw, p, phi):
 def test_cfl_guard_stops_run_steps(cuda):
     cfg = small_cfg()
     uvw, p, phi = O.make_initial_state(cfg, seed=41, noise=0.05)
-    cfg.maxcfl = _limit_after_first_step(cfg, uvw, p, phi)
+    cfg.maxcfl = float(_limit_after_first_step(cfg, uvw, p, phi))
     sol = O.OracleSolver(cfg, uvw, p, phi)
     while sol.isforward:
         sol.run_step()
@@ -74,7 +74,7 @@ def test_cfl_guard_stops_the_main_program(cuda, tmp_path):
     driver = tbuild.build_driver()
     cfg = small_cfg()
     uvw, p, phi = O.make_initial_state(cfg, seed=42, noise=0.05)
-    cfg.maxcfl = _limit_after_first_step(cfg, uvw, p, phi)
+    cfg.maxcfl = float(_limit_after_first_step(cfg, uvw, p, phi))
     write_ini(tmp_path / "configuration.ini", cfg, maxstep=50, writeinterval=50)
     O.write_phase_file(str(tmp_path / "0" / "phase_00_variable.dat"), [uvw, p])
     O.write_phase_file(str(tmp_path / "0" / "phase_01_variable.dat"), [phi])

@@ -24,19 +24,21 @@ KP = 256
 
 
 def _split(M, S):
-    """Slices of the rows of M (each row scaled by 2^e, |row 2^-e| <= 1)."""
+    """Slices of the rows of M (each row scaled by 2^e, |row 2^-e| <= 1): the
+    row on the grid 2^-(6+7(S-1)) of its scale (one rounding, ties to even),
+    then its signed base-128 digits in [-64, 63] from the last slice up, the
+    rest in slice 0."""
     mx = np.max(np.abs(M), axis=1)
     f, e = np.frexp(np.where(mx > 0, mx, 1.0))
     e = np.where(mx > 0, np.where(f == 0.5, e - 1, e), 0)
-    r = np.ldexp(M, -e[:, None])
-    out = []
-    q = np.rint(r * 64.0)
-    out.append(q)
-    r = r * 64.0 - q
-    for _ in range(1, S):
-        q = np.rint(r * 128.0)
-        out.append(q)
-        r = r * 128.0 - q
+    n = np.rint(np.ldexp(M, -e[:, None]) * 2.0 ** (6 + 7 * (S - 1))).astype(np.int64)
+    out = [None] * S
+    for p in range(S - 1, 0, -1):
+        d = ((n + 64) & 127) - 64
+        n = (n - d) >> 7
+        out[p] = d.astype(np.float64)
+    out[0] = n.astype(np.float64)
+    assert all(np.abs(q).max() <= 64 for q in out)
     return out, e
 
 
@@ -51,7 +53,7 @@ def islice_model(A, X):
     for d in range(S):
         Dd = sum(As[p] @ Xs[d - p].T for p in range(d + 1))   # exact: integers below 2^53
         assert np.abs(Dd).max() < 2 ** 31
-        acc = Dd * np.ldexp(1.0, -(12 + 7 * d)) + acc        # exact product, one rounding
+        acc = Dd * np.ldexp(1.0, -(12 + 7 * d)) + acc        # exact: the sum stays below 2^53 units
     interior = acc * np.ldexp(1.0, ae)[:, None] * np.ldexp(1.0, xe)[None, :]
     return (A[:, :1] * X[:1] + interior) + A[:, nz - 1:] * X[nz - 1:]
 

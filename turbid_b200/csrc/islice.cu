@@ -12,12 +12,13 @@
 //   * the operator by rows and the data by columns, over the interior rows
 //     k = 1 .. nz-2 only, into S slices of integers of magnitude <= 64, each
 //     row / column scaled by a power of two 2^e with e from frexp of its
-//     largest magnitude (|x| 2^-e <= 1): slice 0 = rint(64 r), slice p > 0 =
-//     rint(128 r') of the remainder r' -- every step exact in FP64;
+//     largest magnitude (|x| 2^-e <= 1): n = rint(x 2^-e 2^(6+7(S-1)))
+//     (the only rounding), then n's signed base-128 digits in [-64, 63] from
+//     the last slice up, the rest (in [-64, 64]) in slice 0;
 //   * the slice pairs (p, q) with p + q < S multiplied exactly in int32, one
 //     tensor-memory accumulator per diagonal d = p + q;
-//   * the diagonals combined in FP64 with weight 2^-(12+7d), d ascending (one
-//     fma each, exact product), then the row and column scales;
+//   * the diagonals combined with weight 2^-(12+7d): exactly, as one int64
+//     sum (below 2^53) converted to FP64, then the row and column scales;
 //   * the two boundary rows of the data (z = 0 and z = nz-1; the scalar's
 //     Robin rows carry values scaled by 1e7) as an FP64 rank-2 update:
 //     out = (A[r][0] x0 + interior) + A[r][nz-1] x_{nz-1}.
@@ -48,7 +49,7 @@ namespace {
 
 constexpr int KP = 256;                 // interior rows padded to 8 MMA K-steps of 32
 constexpr int BM = 128;                 // data columns per CTA (MMA M, tensor-memory lanes)
-constexpr int kThreads = 128;
+constexpr int kGemmThreads = 512;        // 16 warps: 4 per lane quarter of the accumulators
 constexpr int kTileX = BM * KP;         // bytes of one data tile
 constexpr int kBadExp = INT_MIN;        // column exponent of a column holding NaN or inf
 constexpr long long kSpin = 1ll << 22;  // polls of a bounded wait (each try_wait may suspend)
@@ -57,27 +58,38 @@ template <int S>
 struct IslShape {
   static constexpr int BN = S <= 5 ? 96 : (S == 6 ? 80 : 64);   // S * BN accumulator columns <= 512
   static constexpr int kTileA = BN * KP;
-  static constexpr size_t kSmem = (size_t)S * kTileX + 2 * (size_t)kTileA;
+  static constexpr int kRowsMax = 288;   // rows of the padded operator (nz <= 258 and BN = 96: 3 chunks)
+  static constexpr size_t kSmem = 1024 + (size_t)S * kTileX + 2 * (size_t)kTileA + 4 * kRowsMax * sizeof(double);
+  static_assert(kTileA % 2048 == 0, "half tiles must keep 1024-byte atom alignment");
   static_assert(S * BN <= 512, "one accumulator per slice diagonal must fit tensor memory");
   static_assert(BN % 16 == 0 && BN >= 16 && BN <= 256, "MMA N for M = 128");
 };
 
-__host__ __device__ constexpr int kmaj_off(int row, int k) {
-  return (row >> 3) * (KP / 16) * 128 + (k >> 4) * 128 + (row & 7) * 16 + (k & 15);
+// Byte offset of element (row, k) in a tile of `rows` rows, K-major with the
+// 128-byte swizzle: the K range is cut into two 128-byte halves stored one
+// after the other; within a half, 8-row atoms of 8 x 128 bytes lie 1024 bytes
+// apart and the 16-byte chunk c of row r of an atom sits at chunk c ^ (r & 7)
+// (so the tensor cores' and the slicer's accesses spread over all banks).
+__host__ __device__ constexpr int ksw_off(int rows, int row, int k) {
+  return (k >> 7) * (rows * 128) + (row >> 3) * 1024 + (row & 7) * 128 + ((((k & 127) >> 4) ^ (row & 7)) << 4) +
+         (k & 15);
 }
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
 
-// shared-memory matrix descriptor: canonical K-major layout, no swizzle
-__device__ __forceinline__ uint64_t smem_desc(uint32_t saddr) {
+// shared-memory matrix descriptor of a K-major, 128-byte-swizzled tile of
+// `rows` rows (1024-byte aligned), at the MMA K-step kk (32 bytes of K each)
+__device__ __forceinline__ uint64_t smem_desc(uint32_t tile, int rows, int kk) {
+  const uint32_t saddr = tile + (uint32_t)(kk >> 2) * (uint32_t)(rows * 128) + (uint32_t)(kk & 3) * 32u;
   uint64_t d = 0;
-  d |= (uint64_t)((saddr >> 4) & 0x3FFF);                        // start address
-  d |= (uint64_t)((128 >> 4) & 0x3FFF) << 16;                    // leading byte offset: K chunks
-  d |= (uint64_t)((((KP / 16) * 128) >> 4) & 0x3FFF) << 32;      // stride byte offset: 8-row groups
-  d |= (uint64_t)1 << 46;                                        // descriptor version (sm_100)
-  return d;                                                      // base offset 0, no swizzle
+  d |= (uint64_t)((saddr >> 4) & 0x3FFF);   // start address
+  d |= (uint64_t)1 << 16;                   // leading byte offset (unused with the swizzle; 16 bytes)
+  d |= (uint64_t)(1024 >> 4) << 32;         // stride byte offset: 8-row atoms
+  d |= (uint64_t)1 << 46;                   // descriptor version (sm_100)
+  d |= (uint64_t)2 << 61;                   // layout: 128-byte swizzle
+  return d;                                 // base offset 0 (atoms 1024-byte aligned)
 }
 
 // instruction descriptor: s32 accumulator, signed 8-bit A and B, both K-major
@@ -115,6 +127,11 @@ __device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t
 
 __device__ __forceinline__ double max_keep_nan(double a, double b) { return (b > a || isnan(b)) ? b : a; }
 
+// 2^(6 + 7 (S - 1)): the grid of the last slice (slice 0 holds 6 bits and a
+// sign, every further slice 7 bits and a sign)
+template <int S>
+constexpr double kGrid = (double)(1ll << (6 + 7 * (S - 1)));
+
 // ---------------------------------------------------------------------------
 // Data slicing: four threads per column of a 128-column tile (512 threads).
 // Each finds the maximum magnitude over a quarter of the interior rows; the
@@ -139,7 +156,11 @@ __global__ void __launch_bounds__(kSliceThreads) k_slice_data(const SliceArgs a)
   const int tile = blockIdx.x, pb = blockIdx.y;
   const int c = tile * BM + t;
   const bool valid = c < a.ncol;
-  const double* X = a.in[pb];
+  // select the problem's pointers without indexing the parameter arrays
+  // dynamically (that would copy them to local memory)
+  const double* X = pb == 0 ? a.in[0] : (pb == 1 ? a.in[1] : a.in[2]);
+  int8_t* xs = pb == 0 ? a.xs[0] : (pb == 1 ? a.xs[1] : a.xs[2]);
+  int* xe = pb == 0 ? a.xe[0] : (pb == 1 ? a.xe[1] : a.xe[2]);
   const int nin = a.nz - 2;                       // interior rows z = 1 .. nz-2
   const int z0 = 1 + part * ((nin + 3) / 4), z1 = min(a.nz - 1, z0 + (nin + 3) / 4);
   double mx = 0.0;
@@ -155,8 +176,8 @@ __global__ void __launch_bounds__(kSliceThreads) k_slice_data(const SliceArgs a)
     const double f = frexp(mx, &ee);
     e = f == 0.5 ? ee - 1 : ee;
   }
-  if (valid && part == 0) a.xe[pb][tile * BM + t] = bad ? kBadExp : e;
-  int8_t* dst = a.xs[pb] + (size_t)tile * S * kTileX;
+  if (valid && part == 0) xe[tile * BM + t] = bad ? kBadExp : e;
+  int8_t* dst = xs + (size_t)tile * S * kTileX;
   for (int kc = part * 4; kc < part * 4 + 4; ++kc) {
     uint32_t w[S][4];
 #pragma unroll
@@ -167,20 +188,20 @@ __global__ void __launch_bounds__(kSliceThreads) k_slice_data(const SliceArgs a)
     for (int kk = 0; kk < 16; ++kk) {
       const int z = kc * 16 + kk + 1;
       const double x = (valid && !bad && z < a.nz - 1) ? X[(size_t)z * a.ncol + c] : 0.0;
-      double r = ldexp(x, -e);
-      double q = rint(r * 64.0);
-      r = r * 64.0 - q;
-      w[0][kk >> 2] |= ((uint32_t)(__double2int_rn(q) & 0xff)) << (8 * (kk & 3));
+      // the column value on the 2^-(6+7(S-1)) grid of its scale, then its
+      // signed base-128 digits from the last one up (exact integer steps)
+      long long n = __double2ll_rn(ldexp(x, -e) * kGrid<S>);
 #pragma unroll
-      for (int p = 1; p < S; ++p) {
-        q = rint(r * 128.0);
-        r = r * 128.0 - q;
-        w[p][kk >> 2] |= ((uint32_t)(__double2int_rn(q) & 0xff)) << (8 * (kk & 3));
+      for (int p = S - 1; p >= 1; --p) {
+        const int dg = (int)(((n + 64) & 127) - 64);
+        n = (n - dg) >> 7;
+        w[p][kk >> 2] |= ((uint32_t)(dg & 0xff)) << (8 * (kk & 3));
       }
+      w[0][kk >> 2] |= ((uint32_t)((int)n & 0xff)) << (8 * (kk & 3));
     }
 #pragma unroll
     for (int p = 0; p < S; ++p)
-      *reinterpret_cast<uint4*>(dst + (size_t)p * kTileX + kmaj_off(t, kc * 16)) =
+      *reinterpret_cast<uint4*>(dst + (size_t)p * kTileX + ksw_off(BM, t, kc * 16)) =
           make_uint4(w[p][0], w[p][1], w[p][2], w[p][3]);
   }
 }
@@ -202,64 +223,85 @@ struct IslArgs {
   int* err;
 };
 
+// One CTA per 128 data columns, 16 warps.  Thread 0 issues the bulk copies
+// and the MMAs; the operator is streamed in half tiles (BN rows x 128 bytes of
+// K, one contiguous block of the swizzled tile) through four buffers, three
+// copies ahead of the MMAs.  After each chunk of BN operator rows all warps
+// read the accumulators: warp w reads tensor-memory lanes 32 (w % 4) .. +31
+// (data columns) and every fourth 8-row group of the chunk starting at w / 4.
 template <int S>
-__global__ void __launch_bounds__(kThreads, 1) k_islice_gemm(const IslArgs args) {
+__global__ void __launch_bounds__(kGemmThreads, 1) k_islice_gemm(const IslArgs args) {
   using Sh = IslShape<S>;
   constexpr int BN = Sh::BN;
+  constexpr int kHalf = Sh::kTileA / 2;               // bytes of one half tile
+  constexpr int NBUF = 4;
   constexpr uint32_t idesc = idesc_i8(BM, BN);
-  extern __shared__ __align__(1024) uint8_t sm[];
+  extern __shared__ __align__(16) uint8_t sm_raw[];
+  // swizzle atoms need 1024-byte alignment: round the base up (1 KB reserved)
+  uint8_t* sm = sm_raw + ((1024 - (smem_u32(sm_raw) & 1023)) & 1023);
   uint8_t* sx = sm;                                   // S data tiles
-  uint8_t* sa = sm + (size_t)S * kTileX;              // two operator tiles
-  __shared__ __align__(8) uint64_t bars[6];           // 0 data, 1-2 full, 3-4 empty, 5 accumulators
+  uint8_t* sa = sm + (size_t)S * kTileX;              // four operator half tiles
+  double* s_aux = reinterpret_cast<double*>(sa + NBUF * kHalf);   // a0, an, asc, lam: 4 x kRowsMax
+  __shared__ __align__(8) uint64_t bars[2 + 2 * NBUF];  // data, accumulators, full[4], empty[4]
   __shared__ uint32_t tmem_slot;
   __shared__ int s_err;
-  const int tid = threadIdx.x, warp = tid >> 5;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int tile = blockIdx.x;
   const IslProblem& a = args.p[blockIdx.y];
-  const uint32_t bar_x = smem_u32(&bars[0]), bar_acc = smem_u32(&bars[5]);
-  auto bar_full = [&](int i) { return smem_u32(&bars[1 + i]); };
-  auto bar_empty = [&](int i) { return smem_u32(&bars[3 + i]); };
-  const int total = args.nchunks * S;   // (chunk, operator slice) iterations
+  const uint32_t bar_x = smem_u32(&bars[0]), bar_acc = smem_u32(&bars[1]);
+  auto bar_full = [&](int i) { return smem_u32(&bars[2 + i]); };
+  auto bar_empty = [&](int i) { return smem_u32(&bars[2 + NBUF + i]); };
+  const int total = args.nchunks * S * 2;   // (chunk, operator slice, K half) iterations
 
   if (tid == 0) {
     s_err = 0;
-    for (int i = 0; i < 6; ++i) mbar_init(smem_u32(&bars[i]), 1);
+    for (int i = 0; i < 2 + 2 * NBUF; ++i) mbar_init(smem_u32(&bars[i]), 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(smem_u32(&tmem_slot)));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
+  // per-row epilogue constants: boundary columns, row scale, eigenvalue
+  const int rows_pad = args.nchunks * BN;
+  for (int r = tid; r < rows_pad; r += kGemmThreads) {
+    s_aux[r] = a.a0[r];
+    s_aux[Sh::kRowsMax + r] = a.an[r];
+    s_aux[2 * Sh::kRowsMax + r] = a.asc[r];
+    s_aux[3 * Sh::kRowsMax + r] = (a.ep.mode == EPI_RSCALE && r < args.nz) ? a.ep.lam[r] : 0.0;
+  }
   asm volatile("tcgen05.fence::before_thread_sync;");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;");
   const uint32_t tmem = tmem_slot;
 
-  // bulk loads issued per operator buffer, so that an early exit can drain them
-  int nload[2] = {0, 0};
+  // operator loads issued (load i goes to buffer i % NBUF), so that an early
+  // exit can drain them
+  int issued = 0;
   auto issue_op_load = [&](int it) {
-    const int buf = it & 1;
-    const int8_t* src = a.as + (size_t)it * Sh::kTileA;   // chunk-major, slice-minor = iteration order
-    mbar_expect_tx(bar_full(buf), Sh::kTileA);
-    bulk_g2s(smem_u32(sa + buf * Sh::kTileA), src, Sh::kTileA, bar_full(buf));
-    ++nload[buf];
+    const int buf = it % NBUF;
+    // iteration order = chunk-major, slice, K half: the half tiles lie in that order
+    const int8_t* src = a.as + (size_t)it * kHalf;
+    mbar_expect_tx(bar_full(buf), kHalf);
+    bulk_g2s(smem_u32(sa + buf * kHalf), src, kHalf, bar_full(buf));
+    issued = it + 1;
   };
   if (tid == 0) {
     mbar_expect_tx(bar_x, S * kTileX);
     for (int p = 0; p < S; ++p)
       bulk_g2s(smem_u32(sx + p * kTileX), a.xs + ((size_t)tile * S + p) * kTileX, kTileX, bar_x);
-    issue_op_load(0);
-    if (total > 1) issue_op_load(1);
+    for (int i = 0; i < NBUF - 1 && i < total; ++i) issue_op_load(i);
     if (!mbar_wait(bar_x, 0)) s_err = 1;
   }
 
-  // per-thread column constants
+  // per-thread column constants: this thread's lane quarter and column
   const int ncol = args.ncol, nz = args.nz;
-  const int c = tile * BM + tid;
+  const int quarter = warp & 3, rgrp = warp >> 2;   // rows: 8-row groups rgrp, rgrp + 4, ...
+  const int c = tile * BM + quarter * 32 + lane;
   const bool valid = c < ncol;
   const double xb = valid ? a.in[c] : 0.0;
   const double xt = valid ? a.in[(size_t)(nz - 1) * ncol + c] : 0.0;
-  const int e = valid ? a.xe[tile * BM + tid] : 0;
+  const int e = valid ? a.xe[tile * BM + quarter * 32 + lane] : 0;
   const bool bad = e == kBadExp;
   const double csc = bad ? 0.0 : ldexp(1.0, e);
   const int m = c >> 1;
@@ -270,40 +312,43 @@ __global__ void __launch_bounds__(kThreads, 1) k_islice_gemm(const IslArgs args)
   int it = 0;
   for (int j = 0; j < args.nchunks; ++j) {
     if (tid == 0 && !s_err) {
-      for (int p = 0; p < S; ++p, ++it) {
-        const int buf = it & 1;
-        if (!mbar_wait(bar_full(buf), (it >> 1) & 1)) {
-          s_err = 1;
-          break;
-        }
-        asm volatile("tcgen05.fence::after_thread_sync;");
-        const uint32_t sa_addr = smem_u32(sa + buf * Sh::kTileA);
-        for (int q = 0; q < S - p; ++q) {
-          const uint32_t dacc = tmem + (uint32_t)((p + q) * BN);
-          const uint32_t sx_addr = smem_u32(sx + q * kTileX);
-#pragma unroll
-          for (int kk = 0; kk < KP / 32; ++kk) {
-            const uint64_t da = smem_desc(sx_addr + kk * 256);
-            const uint64_t db = smem_desc(sa_addr + kk * 256);
-            const uint32_t acc = (p == 0 && kk == 0) ? 0u : 1u;   // p = 0 opens every diagonal
-            asm volatile(
-                "{\n\t.reg .pred pd;\n\t"
-                "setp.ne.b32 pd, %4, 0;\n\t"
-                "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, pd;\n\t}" ::"r"(dacc),
-                "l"(da), "l"(db), "r"(idesc), "r"(acc));
-          }
-        }
-        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-            bar_empty(buf)));
-        // refill the other buffer for the next iteration once the MMAs that read it are done
-        const int next = it + 1;
-        if (next >= 2 && next < total) {
-          if (!mbar_wait(bar_empty(next & 1), ((next - 2) >> 1) & 1)) {
+      for (int p = 0; p < S && !s_err; ++p) {
+        for (int h = 0; h < 2; ++h, ++it) {
+          const int buf = it % NBUF;
+          if (!mbar_wait(bar_full(buf), (it / NBUF) & 1)) {
             s_err = 1;
             ++it;
             break;
           }
-          issue_op_load(next);
+          asm volatile("tcgen05.fence::after_thread_sync;");
+          const uint32_t sa_addr = smem_u32(sa + buf * kHalf);
+          for (int q = 0; q < S - p; ++q) {
+            const uint32_t dacc = tmem + (uint32_t)((p + q) * BN);
+            const uint32_t sx_addr = smem_u32(sx + q * kTileX);
+#pragma unroll
+            for (int kl = 0; kl < 4; ++kl) {
+              const uint64_t da = smem_desc(sx_addr, BM, 4 * h + kl);
+              const uint64_t db = smem_desc(sa_addr, BN, kl);
+              const uint32_t acc = (p == 0 && h == 0 && kl == 0) ? 0u : 1u;   // p = 0 opens every diagonal
+              asm volatile(
+                  "{\n\t.reg .pred pd;\n\t"
+                  "setp.ne.b32 pd, %4, 0;\n\t"
+                  "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, pd;\n\t}" ::"r"(dacc),
+                  "l"(da), "l"(db), "r"(idesc), "r"(acc));
+            }
+          }
+          asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+              bar_empty(buf)));
+          // refill the buffer of the previous iteration, NBUF - 1 iterations ahead
+          const int next = it + NBUF - 1;
+          if (next < total) {
+            if (it >= 1 && !mbar_wait(bar_empty((it - 1) % NBUF), ((it - 1) / NBUF) & 1)) {
+              s_err = 1;
+              ++it;
+              break;
+            }
+            issue_op_load(next);
+          }
         }
       }
       asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar_acc));
@@ -316,41 +361,55 @@ __global__ void __launch_bounds__(kThreads, 1) k_islice_gemm(const IslArgs args)
     if (ok) {
       const int r0 = j * BN;
 #pragma unroll 1
-      for (int jg = 0; jg < BN; jg += 16) {
-        double acc[16];
+      for (int jg = rgrp * 8; jg < BN; jg += 32) {
+        // the S diagonals' accumulators of 8 rows, all loads in flight before one wait
+        uint32_t v[S][8];
 #pragma unroll
-        for (int i = 0; i < 16; ++i) acc[i] = 0.0;
-#pragma unroll 1
         for (int d = 0; d < S; ++d) {
-          uint32_t v[16];
-          const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(d * BN + jg);
-          asm volatile(
-              "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
-              "[%16];"
-              : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
-                "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
-                "=r"(v[15])
-              : "r"(taddr));
-          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-          const double w = ldexp(1.0, -(12 + 7 * d));
+          const uint32_t taddr = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(d * BN + jg);
+          asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                       : "=r"(v[d][0]), "=r"(v[d][1]), "=r"(v[d][2]), "=r"(v[d][3]), "=r"(v[d][4]), "=r"(v[d][5]),
+                         "=r"(v[d][6]), "=r"(v[d][7])
+                       : "r"(taddr));
+        }
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        // RSCALE: the reciprocal of a row pair is computed once per mode, the
+        // even lane of a (re, im) lane pair taking the first row and the odd
+        // lane the second, and exchanged
+        double Rpair[8];
+        if (rscale) {
 #pragma unroll
-          for (int i = 0; i < 16; ++i) acc[i] = __fma_rn((double)(int)v[i], w, acc[i]);
+          for (int i = 0; i < 8; i += 2) {
+            const int rm = r0 + jg + i + (lane & 1);
+            double R = 1.0;
+            if (rm != 0 && rm < nz - 1) {
+              const double lam = s_aux[3 * Sh::kRowsMax + rm];
+              R = __drcp_rn((k2m + lam) + a.ep.sigma);   // correctly rounded 1 / x
+              if (a.ep.null_mode && m == 0 && fabs(lam) < 10e-12) R = 0.0;
+            }
+            const double Ro = __shfl_xor_sync(0xffffffffu, R, 1);
+            Rpair[i] = (lane & 1) ? Ro : R;
+            Rpair[i + 1] = (lane & 1) ? R : Ro;
+          }
         }
         if (valid) {
 #pragma unroll
-          for (int i = 0; i < 16; ++i) {
+          for (int i = 0; i < 8; ++i) {
             const int r = r0 + jg + i;
+            // sum_d D_d 2^-(12+7d) = 2^-(12+7(S-1)) sum_d D_d 2^(7(S-1-d)): an
+            // integer below 2^53 in magnitude (|D_d| <= (d+1) 2^20), so the
+            // int64 sum and its conversion to FP64 are exact
+            long long isum = (int)v[0][i];
+#pragma unroll
+            for (int d = 1; d < S; ++d) isum = isum * 128 + (int)v[d][i];
+            const double acc = __ll2double_rn(isum) * (1.0 / (double)(1ll << (12 + 7 * (S - 1))));
             if (r < args.nrow) {
-              const double interior = __dmul_rn(__dmul_rn(acc[i], __ldg(a.asc + r)), csc);
-              double v = __dadd_rn(__dadd_rn(__dmul_rn(__ldg(a.a0 + r), xb), interior), __dmul_rn(__ldg(a.an + r), xt));
-              if (bad) v = __longlong_as_double(0x7ff8000000000000LL);
-              if (rscale && r != 0 && r != nz - 1) {
-                const double lam = __ldg(a.ep.lam + r);
-                double R = 1.0 / ((k2m + lam) + a.ep.sigma);
-                if (a.ep.null_mode && m == 0 && fabs(lam) < 10e-12) R = 0.0;
-                v = __dmul_rn(v, R);
-              }
-              out[(size_t)r * ncol + c] = v;
+              const double interior = __dmul_rn(__dmul_rn(acc, s_aux[2 * Sh::kRowsMax + r]), csc);
+              double val = __dadd_rn(__dadd_rn(__dmul_rn(s_aux[r], xb), interior),
+                                     __dmul_rn(s_aux[Sh::kRowsMax + r], xt));
+              if (bad) val = __longlong_as_double(0x7ff8000000000000LL);
+              if (rscale) val = __dmul_rn(val, Rpair[i]);
+              out[(size_t)r * ncol + c] = val;
             }
           }
         }
@@ -364,8 +423,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_islice_gemm(const IslArgs args)
   // released (the MMAs were awaited through the accumulator barrier)
   if (tid == 0 && s_err) {
     mbar_wait(bar_x, 0);
-    for (int k = 0; k < 2; ++k)
-      if (nload[k] > 0) mbar_wait(bar_full(k), (nload[k] - 1) & 1);
+    for (int k = 0; k < NBUF && k < issued; ++k) {
+      const int nk = (issued - 1 - k) / NBUF + 1;   // loads into buffer k
+      mbar_wait(bar_full(k), (nk - 1) & 1);
+    }
     atomicExch(args.err, 1);
   }
   __syncthreads();
@@ -418,16 +479,15 @@ static void slice_operator_host(const std::vector<double>& A, int nrow, int nz, 
     aux[rows_pad + r] = A[(size_t)r * nz + nz - 1];
     aux[2 * rows_pad + r] = std::ldexp(1.0, e);
     const int j = r / BN, rr = r % BN;
+    const double grid = std::ldexp(1.0, 6 + 7 * (S - 1));
     for (int k = 0; k + 1 < nz - 1; ++k) {
-      double x = std::ldexp(A[(size_t)r * nz + k + 1], -e);
-      double q = std::rint(x * 64.0);
-      x = x * 64.0 - q;
-      tiles[((size_t)j * S + 0) * BN * KP + kmaj_off(rr, k)] = (int8_t)(int)q;
-      for (int p = 1; p < S; ++p) {
-        q = std::rint(x * 128.0);
-        x = x * 128.0 - q;
-        tiles[((size_t)j * S + p) * BN * KP + kmaj_off(rr, k)] = (int8_t)(int)q;
+      long long n = std::llrint(std::ldexp(A[(size_t)r * nz + k + 1], -e) * grid);   // ties to even
+      for (int p = S - 1; p >= 1; --p) {
+        const int dg = (int)(((n + 64) & 127) - 64);
+        n = (n - dg) >> 7;
+        tiles[((size_t)j * S + p) * BN * KP + ksw_off(BN, rr, k)] = (int8_t)dg;
       }
+      tiles[((size_t)j * S + 0) * BN * KP + ksw_off(BN, rr, k)] = (int8_t)n;
     }
   }
 }
@@ -517,7 +577,7 @@ void islice_group(const IsliceOp* const* ops, const double2* const* ins, double2
   prof_begin(s, PC_GEMM, by, fl, fl);
   k_slice_data<5><<<dim3(op0.ntiles, n), kSliceThreads, 0, s>>>(sa);
   TG_LAUNCH_CHECK("k_slice_data");
-  k_islice_gemm<5><<<dim3(op0.ntiles, n), kThreads, Sh::kSmem, s>>>(a);
+  k_islice_gemm<5><<<dim3(op0.ntiles, n), kGemmThreads, Sh::kSmem, s>>>(a);
   prof_end(s);
   TG_LAUNCH_CHECK("k_islice_gemm");
 }
