@@ -99,7 +99,8 @@ struct Ctx {
   int* yidx = nullptr;
   ZOperator opD1, opD2, opTmp, opEinv[5], opE[5];
   // z-solver of the dense Helmholtz solves in mixed precision: FP64 DMMA
-  // (TG_ZSOLVER_DMMA) or the int8-slice tensor-core product (TG_ZSOLVER_ISLICE)
+  // (TG_ZSOLVER_DMMA) or the int8-slice tensor-core product (TG_ZSOLVER_ISLICE,
+  // the default of the mixed mode)
   int zsolver = TG_ZSOLVER_DMMA;
   IsliceOp* islTmp = nullptr;
   double* lamd[5] = {nullptr};
@@ -253,6 +254,8 @@ static Ctx* create(const tg_case& c) {
   x.S = (size_t)x.nz * x.M;
   x.P = (size_t)x.nx * x.ny * x.nz;
   x.mixed = c.precision == TG_PREC_MIXED;
+  // mixed precision: the dense solves on the int8-slice tensor-core product
+  x.zsolver = x.mixed ? TG_ZSOLVER_ISLICE : TG_ZSOLVER_DMMA;
   x.scalar = c.nphase > 1;
   x.opentop = std::fabs(c.bc_u[2] - 0) <= kSmall && std::fabs(c.bc_u[3] - 1) <= kSmall;  // boundary.cc:59-71
   x.dt = c.dt;

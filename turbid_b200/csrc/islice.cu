@@ -131,44 +131,54 @@ __device__ __forceinline__ double max_keep_nan(double a, double b) { return (b >
 // sign, every further slice 7 bits and a sign)
 template <int S>
 constexpr double kGrid = (double)(1ll << (6 + 7 * (S - 1)));
+// 64 (1 + 128 + ... + 128^(S-2)): makes the digits of slices 1 .. S-1 non-negative
+template <int S>
+constexpr long long kBias = (S <= 1) ? 0 : 64 * (((1ll << (7 * (S - 1))) - 1) / 127);
 
 // ---------------------------------------------------------------------------
-// Data slicing: four threads per column of a 128-column tile (512 threads).
-// Each finds the maximum magnitude over a quarter of the interior rows; the
-// column's exponent follows from their maximum; then each writes the S slices
-// of a quarter of the K range in the tile image order (16 K values = one
-// 16-byte chunk at a time).  blockIdx.y selects the problem of a group.
+// Data slicing: a CTA of 16 warps slices 32 columns; warp q reads the 16
+// interior rows of K chunk q (rows 16 q + 1 .. 16 q + 16) of its 32 columns
+// (lane = column: 256 contiguous bytes per row), keeps them in registers, the
+// column maxima meet in shared memory, and each warp writes the S slices of
+// its K chunk into the column tile's image (16 bytes per column and slice).
+// blockIdx.y selects the problem of a group.
 // ---------------------------------------------------------------------------
 constexpr int kMaxIsl = 3;
-constexpr int kSliceThreads = 4 * BM;
+constexpr int kSliceCols = 32;
+constexpr int kSliceThreads = kSliceCols * (KP / 16);   // 512
 
 struct SliceArgs {
   const double* in[kMaxIsl];   // FP64 component, row-major [nz][ncol]
   int8_t* xs[kMaxIsl];         // data tiles [tile][S][kTileX]
   int* xe[kMaxIsl];            // column exponents [tile * 128 + i]
-  int nz, ncol, ntiles;
+  int nz, ncol;
 };
 
 template <int S>
 __global__ void __launch_bounds__(kSliceThreads) k_slice_data(const SliceArgs a) {
-  __shared__ double part_max[4][BM];
-  const int t = threadIdx.x & (BM - 1), part = threadIdx.x >> 7;
-  const int tile = blockIdx.x, pb = blockIdx.y;
-  const int c = tile * BM + t;
+  __shared__ double part_max[KP / 16][kSliceCols];
+  const int lane = threadIdx.x & 31, kc = threadIdx.x >> 5;   // column in the block, K chunk
+  const int pb = blockIdx.y;
+  const int c = blockIdx.x * kSliceCols + lane;
   const bool valid = c < a.ncol;
   // select the problem's pointers without indexing the parameter arrays
   // dynamically (that would copy them to local memory)
   const double* X = pb == 0 ? a.in[0] : (pb == 1 ? a.in[1] : a.in[2]);
   int8_t* xs = pb == 0 ? a.xs[0] : (pb == 1 ? a.xs[1] : a.xs[2]);
   int* xe = pb == 0 ? a.xe[0] : (pb == 1 ? a.xe[1] : a.xe[2]);
-  const int nin = a.nz - 2;                       // interior rows z = 1 .. nz-2
-  const int z0 = 1 + part * ((nin + 3) / 4), z1 = min(a.nz - 1, z0 + (nin + 3) / 4);
+  double x[16];
   double mx = 0.0;
-  if (valid)
-    for (int z = z0; z < z1; ++z) mx = max_keep_nan(mx, fabs(X[(size_t)z * a.ncol + c]));
-  part_max[part][t] = mx;
+#pragma unroll
+  for (int kk = 0; kk < 16; ++kk) {
+    const int z = kc * 16 + kk + 1;
+    x[kk] = (valid && z < a.nz - 1) ? X[(size_t)z * a.ncol + c] : 0.0;
+    mx = max_keep_nan(mx, fabs(x[kk]));
+  }
+  part_max[kc][lane] = mx;
   __syncthreads();
-  mx = max_keep_nan(max_keep_nan(part_max[0][t], part_max[1][t]), max_keep_nan(part_max[2][t], part_max[3][t]));
+  mx = 0.0;
+#pragma unroll
+  for (int q = 0; q < KP / 16; ++q) mx = max_keep_nan(mx, part_max[q][lane]);
   int e = 0;
   const bool bad = !(mx <= DBL_MAX);
   if (!bad && mx > 0.0) {
@@ -176,34 +186,42 @@ __global__ void __launch_bounds__(kSliceThreads) k_slice_data(const SliceArgs a)
     const double f = frexp(mx, &ee);
     e = f == 0.5 ? ee - 1 : ee;
   }
-  if (valid && part == 0) xe[tile * BM + t] = bad ? kBadExp : e;
-  int8_t* dst = xs + (size_t)tile * S * kTileX;
-  for (int kc = part * 4; kc < part * 4 + 4; ++kc) {
-    uint32_t w[S][4];
+  const int tile = c / BM, t = c % BM;   // column tile and column within it
+  if (valid && kc == 0) xe[c] = bad ? kBadExp : e;
+  if (!valid && c >= (a.ncol + BM - 1) / BM * BM) return;   // beyond the last tile
+  uint32_t w[S][4];
 #pragma unroll
-    for (int p = 0; p < S; ++p)
+  for (int p = 0; p < S; ++p)
 #pragma unroll
-      for (int j = 0; j < 4; ++j) w[p][j] = 0u;
+    for (int j = 0; j < 4; ++j) w[p][j] = 0u;
+  // 2^(6+7(S-1)-e) as one exact power-of-two factor when it is a normal
+  // double (any column whose maximum is above 2^-980), else ldexp per value
+  const int sh = 6 + 7 * (S - 1) - e;
+  const bool fast = sh <= 1023;
+  const double scale = fast ? ldexp(1.0, sh) : 0.0;
 #pragma unroll
-    for (int kk = 0; kk < 16; ++kk) {
-      const int z = kc * 16 + kk + 1;
-      const double x = (valid && !bad && z < a.nz - 1) ? X[(size_t)z * a.ncol + c] : 0.0;
-      // the column value on the 2^-(6+7(S-1)) grid of its scale, then its
-      // signed base-128 digits from the last one up (exact integer steps)
-      long long n = __double2ll_rn(ldexp(x, -e) * kGrid<S>);
+  for (int kk = 0; kk < 16; ++kk) {
+    // the column value on the 2^-(6+7(S-1)) grid of its scale (the one
+    // rounding), then its signed base-128 digits: with the bias
+    // 64 (1 + 128 + ... + 128^(S-2)) the digits of slices 1 .. S-1 are the
+    // plain base-128 digits of the low 7 (S-1) bits, less 64, and slice 0 is
+    // the rest (the unique representation the digit-by-digit rule gives)
+    const double xv = bad ? 0.0 : x[kk];
+    const long long n = __double2ll_rn(fast ? xv * scale : ldexp(xv, -e) * kGrid<S>);
+    const long long u = n + kBias<S>;
+    const uint32_t lo = (uint32_t)u;
 #pragma unroll
-      for (int p = S - 1; p >= 1; --p) {
-        const int dg = (int)(((n + 64) & 127) - 64);
-        n = (n - dg) >> 7;
-        w[p][kk >> 2] |= ((uint32_t)(dg & 0xff)) << (8 * (kk & 3));
-      }
-      w[0][kk >> 2] |= ((uint32_t)((int)n & 0xff)) << (8 * (kk & 3));
+    for (int p = 1; p < S; ++p) {
+      const uint32_t dg = ((lo >> (7 * (S - 1 - p))) & 127u) + 0xC0u;   // (digit - 64) as a byte
+      w[p][kk >> 2] |= (dg & 0xffu) << (8 * (kk & 3));
     }
-#pragma unroll
-    for (int p = 0; p < S; ++p)
-      *reinterpret_cast<uint4*>(dst + (size_t)p * kTileX + ksw_off(BM, t, kc * 16)) =
-          make_uint4(w[p][0], w[p][1], w[p][2], w[p][3]);
+    w[0][kk >> 2] |= ((uint32_t)(int)(u >> (7 * (S - 1))) & 0xffu) << (8 * (kk & 3));
   }
+  int8_t* dst = xs + (size_t)tile * S * kTileX;
+#pragma unroll
+  for (int p = 0; p < S; ++p)
+    *reinterpret_cast<uint4*>(dst + (size_t)p * kTileX + ksw_off(BM, t, kc * 16)) =
+        make_uint4(w[p][0], w[p][1], w[p][2], w[p][3]);
 }
 
 struct IslProblem {
@@ -565,7 +583,6 @@ void islice_group(const IsliceOp* const* ops, const double2* const* ins, double2
   }
   sa.nz = op0.nz;
   sa.ncol = op0.ncol;
-  sa.ntiles = op0.ntiles;
   a.nz = op0.nz;
   a.nrow = op0.nrow;
   a.ncol = op0.ncol;
@@ -575,7 +592,7 @@ void islice_group(const IsliceOp* const* ops, const double2* const* ins, double2
   const double by = n * (16.0 * M * op0.nz * 2 + (double)op0.ntiles * 5 * kTileX * 2);
   const double fl = n * 4.0 * op0.nz * op0.nz * (double)M;
   prof_begin(s, PC_GEMM, by, fl, fl);
-  k_slice_data<5><<<dim3(op0.ntiles, n), kSliceThreads, 0, s>>>(sa);
+  k_slice_data<5><<<dim3(op0.ntiles * (BM / kSliceCols), n), kSliceThreads, 0, s>>>(sa);
   TG_LAUNCH_CHECK("k_slice_data");
   k_islice_gemm<5><<<dim3(op0.ntiles, n), kGemmThreads, Sh::kSmem, s>>>(a);
   prof_end(s);
