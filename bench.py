@@ -64,12 +64,18 @@ def replica_rate(steps_per_rank: int, ms_max: float, world: int) -> float:
     return steps_per_rank * world / (ms_max * 1e-3)
 
 
-def ensemble_params(count: int = 16, seed: int = 4) -> list:
-    """Uneven grids and parameters drawn from a seed: Nx = Ny any even length
-    in [64, 192] (lengths with a large prime factor take the transforms'
-    direct-DFT pass), Nz = Nx + 1, Re ~ U[400, 1000], Ws ~ logU[1e-4, 1e-3],
-    Schmidt 0.5."""
-    sizes = list(range(64, 193, 2))
+def ensemble_params(count: int = 16, seed: int = 4, smooth_only: bool = True) -> list:
+    """Uneven grids and parameters drawn from a seed: Nx = Ny even in [64, 192]
+    with prime factors up to 7 (the FFT-friendly lengths a spectral case uses;
+    smooth_only=False draws any even length: the library runs those too, a
+    prime factor above 13 through a direct-DFT pass, several times slower),
+    Nz = Nx + 1, Re ~ U[400, 1000], Ws ~ logU[1e-4, 1e-3], Schmidt 0.5."""
+    def smooth(n):
+        for q in (2, 3, 5, 7):
+            while n % q == 0:
+                n //= q
+        return n == 1
+    sizes = [n for n in range(64, 193, 2) if smooth(n) or not smooth_only]
     rng = np.random.default_rng(seed)
     out = []
     for _ in range(count):
@@ -232,9 +238,11 @@ def fp64_gemm_peak(torch) -> float:
 
 
 def traffic_summary() -> dict:
+    """Per-launch DRAM bytes of each kernel class from the committed ncu
+    captures (profiles/traffic.json; its "note" says which launch each is)."""
     try:
         with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
-            return json.load(f)
+            return {k: v for k, v in json.load(f).items() if k != "note"}
     except Exception:
         return {}
 
@@ -433,9 +441,11 @@ def our_arm(args):
         peak = fp64_gemm_peak(torch)
         achieved = d["flops"] / (d["ms"] * 1e-3) / 1e12
         executed = d.get("xflops", d["flops"]) / (d["ms"] * 1e-3) / 1e12
-        roof = {"kernel": "zgemm_dense_kernel / zgemm_sym_kernel (FP64 DMMA z-operator GEMMs)", "bound": "tensor",
+        roof = {"kernel": "zgemm_dense_kernel / zgemm_sym_kernel (FP64 DMMA z-operator GEMMs; the mixed mode's "
+                          "dense solves run on the int8-slice kernels, class 'islice' of kernels)",
+                "bound": "tensor",
                 "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                "flops": "algorithmic: 4 Nz^2 M per component application (the dense product the reference "
+                "flops": "algorithmic: 4 Nz^2 M per component application (the dense FP64 product the reference "
                          "performs); the folded and split kernels execute about half of that",
                 "executed_tflops": executed, "executed_frac": executed / peak,
                 "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no FP64 figure)",
@@ -457,7 +467,10 @@ def our_arm(args):
         tr = traffic_summary().get(args.workload, {}).get(prec, {}).get(k)
         if tr:
             ent["traffic_per_launch"] = tr
-        if v["flops"]:
+        if v["flops"] and k == "islice":
+            # FP64-equivalent: the dense products these int8 slices stand for
+            ent["fp64_equivalent_TFLOP/s"] = v["flops"] / (v["ms"] * 1e-3) / 1e12
+        elif v["flops"]:
             ent["TFLOP/s"] = v["flops"] / (v["ms"] * 1e-3) / 1e12
             ent["executed_TFLOP/s"] = v.get("xflops", v["flops"]) / (v["ms"] * 1e-3) / 1e12
         kernels[k] = ent

@@ -204,13 +204,15 @@ TG_API tg_status tg_features(tg_ctx* ctx, double* out);
  * tg_profile_begin starts recording CUDA events around every instrumented
  * launch on the context's stream; tg_profile_end synchronizes and returns per
  * class the summed device milliseconds, algorithmic bytes and flops and the
- * launch count.  Classes: 0 z-operator GEMM, 1 forward x pass, 2 forward y
- * pass, 3 backward y pass, 4 backward x pass, 5 elementwise, 6 positivity
- * filter, 7 feature reduction.  The algorithmic flops of a z-operator are
+ * launch count.  Classes: 0 z-operator GEMM (FP64 DMMA), 1 forward x pass,
+ * 2 forward y pass, 3 backward y pass, 4 backward x pass, 5 elementwise,
+ * 6 positivity filter, 7 feature reduction, 8 backward x pass fused with the
+ * advective products (three gradient fields per output), 9 int8-slice
+ * z-operator products (slicing and tensor-core product).  The algorithmic flops of a z-operator are
  * those of the dense product, 4 Nz^2 M per component (the reference's count);
  * tg_profile_executed returns, for the window that tg_profile_end closed, the
  * flops the kernels executed (half of those for folded or split operators). */
-#define TG_PROF_NCAT 8
+#define TG_PROF_NCAT 10
 TG_API tg_status tg_profile_begin(tg_ctx* ctx);
 TG_API tg_status tg_profile_end(tg_ctx* ctx, int ncat, double* ms, double* bytes,
                                 double* flops, int* count);

@@ -52,10 +52,12 @@ def sediment_cfg(**kw):
 # field-container primitives
 # ----------------------------------------------------------------------------
 # powers of two 8..1024 run the in-place radix-16 pass kernels, the other
-# lengths the mixed-radix pass kernels
+# lengths the mixed-radix pass kernels (a prime factor above 13: one direct
+# DFT pass, e.g. 158 = 2 x 79, 106 = 2 x 53, 34 = 2 x 17, 46 = 2 x 23)
 @pytest.mark.parametrize("shape", [(24, 18, 9), (32, 32, 17), (3, 3, 5), (30, 20, 7), (8, 8, 3), (16, 64, 3),
                                    (1024, 16, 3), (8, 1024, 3), (128, 512, 3), (512, 24, 3), (256, 256, 129),
-                                   (64, 64, 5), (256, 64, 3), (512, 128, 3), (64, 512, 3), (512, 256, 3)])
+                                   (64, 64, 5), (256, 64, 3), (512, 128, 3), (64, 512, 3), (512, 256, 3),
+                                   (158, 106, 5), (34, 46, 5)])
 def test_dft_f64_matches_oracle(cuda, shape):
     import torch
     nx, ny, nz = shape
@@ -193,6 +195,12 @@ def test_fp64_steps_with_sediment(cuda):
 def test_fp64_steps_with_sediment_sloped(cuda):
     cfg = sediment_cfg(slope=0.05, slope_direction=1, nx=12, ny=12, nz=17)
     _compare_run(cfg, 11, seed=5, noise=0.05, tol=1e-10)
+
+
+def test_fp64_steps_prime_factor_lengths(cuda):
+    """Nx = 34 (2 x 17) and Ny = 46 (2 x 23): the direct-DFT pass of the
+    mixed-radix transforms in every stage."""
+    _compare_run(sediment_cfg(nx=34, ny=46, nz=17), 2, seed=14, noise=0.05, tol=1e-10)
 
 
 def test_fp64_steps_radix16_transforms(cuda):

@@ -81,7 +81,8 @@ def ensemble_cfgs(count, seed, lo=24, hi=48):
 
 def test_ensemble_matches_single_cases(cuda):
     """tg_run_ensemble (cases on their own streams, stepped together) gives each
-    case exactly the fields of its own tg_run_steps run."""
+    case exactly the fields of its own tg_run_steps run, also over a second
+    call that replays the recorded step graphs."""
     import torch
     cfgs = ensemble_cfgs(4, seed=5)
     precisions = ["mixed", "fp64", "mixed", "mixed"]
@@ -98,9 +99,10 @@ def test_ensemble_matches_single_cases(cuda):
 
     ens = [make(i) for i in range(len(cfgs))]
     assert tb.run_ensemble(ens, 6) == [6] * len(cfgs)
+    assert tb.run_ensemble(ens, 3) == [3] * len(cfgs)
     for i in range(len(cfgs)):
         one = make(i)
-        assert one.run_steps(6) == 6
+        assert one.run_steps(9) == 9
         a, b = ens[i].download_state(), one.download_state()
         for x, y in zip(a, b):
             assert np.array_equal(x, y), i

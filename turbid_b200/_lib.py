@@ -23,9 +23,9 @@ TG_ERR_TIMEOUT = 8
 TG_PREC_FP64 = 0
 TG_PREC_MIXED = 1
 TG_NFEATURE = 50
-TG_PROF_NCAT = 8
+TG_PROF_NCAT = 10
 PROF_NAMES = ["zgemm", "fft_fwd_x", "fft_fwd_y", "fft_bwd_y", "fft_bwd_x", "elementwise", "filter",
-              "features"]
+              "features", "advection_x", "islice"]
 
 _c_d = ctypes.c_double
 _c_i = ctypes.c_int

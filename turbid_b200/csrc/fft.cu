@@ -1031,7 +1031,7 @@ void dft_backward_adv(const TransformDims& d, const FftPlan& px, const FftPlan& 
   {  // x pass and the advection sums
     const size_t P = (size_t)d.nx * d.ny * d.nz;
     // per component: three gradient intermediates in, one field out; the velocity once
-    prof_begin(s, PC_FFT_BX,
+    prof_begin(s, PC_ADV,
                (double)d.nz * d.ny * (ncomp * (3.0 * d.nxh * sizeof(C) + 1.0 * d.nx * sizeof(T)) + 3.0 * d.nx * sizeof(T)),
                0);
     const C* tw = Tw<T>::get(px);

@@ -66,32 +66,35 @@ struct EpiIn {
 
 template <int MODE>
 __device__ __forceinline__ EpiIn epi_load(const EpiParams& ep, int b, int r, int m) {
+  // read-only operands (never the launch's output: every caller passes
+  // separate buffers), loaded through the non-coherent path so that the
+  // compiler may move them ahead of the epilogue's stores
   EpiIn in;
   switch (MODE) {
     case EPI_RSCALE:
       if (r != 0 && r != ep.nz - 1) {
-        in.s1 = ep.lam[r];
-        in.s0 = (ep.k2[m] + in.s1) + ep.sigma;
+        in.s1 = __ldg(ep.lam + r);
+        in.s0 = (__ldg(ep.k2 + m) + in.s1) + ep.sigma;
       }
       break;
     case EPI_DIV: {
       const size_t o = (size_t)b * ep.sX + (size_t)r * ep.M + m;
-      in.a = ep.X0[o];
-      in.c = ep.X1[o];
-      in.s0 = ep.kx[m];
-      in.s1 = ep.ky[m];
+      in.a = __ldg(ep.X0 + o);
+      in.c = __ldg(ep.X1 + o);
+      in.s0 = __ldg(ep.kx + m);
+      in.s1 = __ldg(ep.ky + m);
       break;
     }
     case EPI_LAPRHS:
-      in.a = ep.H[(size_t)b * ep.sH + (size_t)r * ep.M + m];
-      in.c = ep.U[(size_t)b * ep.sU + (size_t)r * ep.M + m];
-      in.s0 = ep.dx2[m];
-      in.s1 = ep.dy2[m];
+      in.a = __ldg(ep.H + (size_t)b * ep.sH + (size_t)r * ep.M + m);
+      in.c = __ldg(ep.U + (size_t)b * ep.sU + (size_t)r * ep.M + m);
+      in.s0 = __ldg(ep.dx2 + m);
+      in.s1 = __ldg(ep.dy2 + m);
       break;
     case EPI_GRAD:
-      in.a = ep.X0[(size_t)b * ep.sX + (size_t)r * ep.M + m];
-      in.s0 = ep.kx[m];
-      in.s1 = ep.ky[m];
+      in.a = __ldg(ep.X0 + (size_t)b * ep.sX + (size_t)r * ep.M + m);
+      in.s0 = __ldg(ep.kx + m);
+      in.s1 = __ldg(ep.ky + m);
       break;
     default:
       break;

@@ -591,7 +591,7 @@ void islice_group(const IsliceOp* const* ops, const double2* const* ins, double2
   a.err = op0.err;
   const double by = n * (16.0 * M * op0.nz * 2 + (double)op0.ntiles * 5 * kTileX * 2);
   const double fl = n * 4.0 * op0.nz * op0.nz * (double)M;
-  prof_begin(s, PC_GEMM, by, fl, fl);
+  prof_begin(s, PC_ISLICE, by, fl, fl);
   k_slice_data<5><<<dim3(op0.ntiles * (BM / kSliceCols), n), kSliceThreads, 0, s>>>(sa);
   TG_LAUNCH_CHECK("k_slice_data");
   k_islice_gemm<5><<<dim3(op0.ntiles, n), kGemmThreads, Sh::kSmem, s>>>(a);

@@ -47,7 +47,7 @@ extern long long g_launches;   // kernel launches issued by this library (host t
 // ---------------------------------------------------------------------------
 // per-kernel-class timing with CUDA events (enabled by tg_profile_begin)
 // ---------------------------------------------------------------------------
-enum ProfCat { PC_GEMM = 0, PC_FFT_FX, PC_FFT_FY, PC_FFT_BY, PC_FFT_BX, PC_ELEM, PC_FILTER, PC_FEAT, PC_N };
+enum ProfCat { PC_GEMM = 0, PC_FFT_FX, PC_FFT_FY, PC_FFT_BY, PC_FFT_BX, PC_ELEM, PC_FILTER, PC_FEAT, PC_ADV, PC_ISLICE, PC_N };
 // flops: algorithmic; xflops: executed (< 0: the same)
 void prof_begin(cudaStream_t s, int cat, double bytes, double flops, double xflops = -1.0);
 void prof_end(cudaStream_t s);
