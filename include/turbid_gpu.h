@@ -279,8 +279,17 @@ TG_API tg_status tg_multiply_islice(tg_ctx* ctx, const double* A_host, const dou
 #define TG_ZSOLVER_ISLICE 1
 TG_API tg_status tg_set_zsolver(tg_ctx* ctx, int solver);
 /* 1 in *flag when a bounded device wait of an int8-slice product gave up
- * since the context was created (the product's output is then invalid). */
+ * since the context was created (the product's output is then invalid).
+ * tg_run_steps checks the same flag with every step's features and stops
+ * with TG_ERR_TIMEOUT when it is set. */
 TG_API tg_status tg_zsolver_error(tg_ctx* ctx, int* flag);
+/* Failure-path check of the int8-slice product (no reference counterpart):
+ * runs one product whose operator copies are withheld, so that its bounded
+ * wait for them gives up; the kernel drains, frees its tensor memory, sets
+ * the flag and returns.  Returns TG_ERR_TIMEOUT when that path worked (the
+ * flag is cleared again; the context stays usable), TG_OK if the wait did
+ * not give up. */
+TG_API tg_status tg_islice_selftest(tg_ctx* ctx);
 /* CmDz2 solve of FlatCarrierPhase::Helmholtz / FlatScalarPhase::Helmholtz
  * (src/phase_carrier_flat.cc:861-994, src/phase_scalar_flat.cc:635-667) for
  * one spectral component: which as in tg_set_decomposition, stage 0..2;

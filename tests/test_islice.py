@@ -7,7 +7,9 @@ boundary rows) reproduces the FP64 product to about 1e-9.
 GPU: tg_multiply_islice equals that model bit for bit (interior rows of at
 most 256, partial 128-column tiles, boundary rows scaled by 1e7, a zero
 column); a mixed-precision run with the int8-slice solves stays within the
-mixed budget (1e-5) of the FP64 path, and no bounded device wait gave up.
+mixed budget (1e-5) of the FP64 path, and no bounded device wait gave up; a
+product whose operator copies are withheld gives up its wait, reports
+TG_ERR_TIMEOUT and leaves the context usable.
 """
 import ctypes
 import math
@@ -166,3 +168,36 @@ def test_mixed_steps_with_islice_solves(cuda, nz):
         e64 = O.rel_l2(runs["islice"][k], runs["fp64"][k])
         emx = O.rel_l2(runs["islice"][k], runs["dmma"][k])
         assert e64 < 1e-5 and emx < 5e-6, (k, e64, emx)
+
+
+@pytest.mark.gpu
+def test_islice_bounded_wait_gives_up_and_context_stays_usable(cuda):
+    """The failure path of the product's bounded waits, without a GPU fault:
+    tg_islice_selftest runs a product whose operator copies are never issued,
+    so the wait for them gives up; the kernel drains, frees its tensor memory,
+    sets the flag and returns, and the call reports TG_ERR_TIMEOUT.  The flag
+    is cleared after it, and the context's steps afterwards equal, bit for bit,
+    those of a context that never ran the check."""
+    nz = 33
+    cfg = O.CaseConfig(nx=24, ny=18, nz=nz, nphase=2, reynolds=800.0, froude=1.0, averaged_concentration=1e-3,
+                       bc_u=[1, 0, 0, 1, 0], bc_v=[1, 0, 0, 1, 0], settling=5e-4, schmidt=0.5,
+                       critical_shear=2e-4, erosion_rate=1e-4, dt=2 * math.pi / 2000)
+    uvw, p, phi = O.make_initial_state(cfg, seed=5, noise=0.05)
+    lib = _lib.load()
+    states = []
+    for selftest in (False, True):
+        gc = _case(24, 18, nz)
+        _lib.check(lib.tg_set_zsolver(gc.h, 1))
+        gc.upload_state(uvw, p, phi)
+        gc.run_steps(2)
+        if selftest:
+            assert lib.tg_islice_selftest(gc.h) == _lib.TG_ERR_TIMEOUT
+            assert b"bounded wait" in lib.tg_last_error()
+            flag = ctypes.c_int(-1)
+            _lib.check(lib.tg_zsolver_error(gc.h, ctypes.byref(flag)))
+            assert flag.value == 0
+        gc.run_steps(3)
+        states.append(gc.download_state())
+        gc.close()
+    for a, b in zip(states[0], states[1]):
+        assert np.array_equal(a, b)

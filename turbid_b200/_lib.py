@@ -108,6 +108,7 @@ _SIGS = [
     ("tg_multiply_islice", _c_i, [_vp, _pd, _vp, _vp, _c_i]),
     ("tg_set_zsolver", _c_i, [_vp, _c_i]),
     ("tg_zsolver_error", _c_i, [_vp, _pi]),
+    ("tg_islice_selftest", _c_i, [_vp]),
     ("tg_helmholtz", _c_i, [_vp, _c_i, _c_i, _vp, _vp]),
 ]
 

@@ -103,6 +103,10 @@ struct Ctx {
   // the default of the mixed mode)
   int zsolver = TG_ZSOLVER_DMMA;
   IsliceOp* islTmp = nullptr;
+  // the flag of the int8-slice products' bounded waits (device), copied to
+  // err_h[slot] with every step's features and checked with them
+  int* isl_err = nullptr;
+  int* err_h = nullptr;   // pinned [2]
   double* lamd[5] = {nullptr};
   FftPlan px, py;
   TransformDims td{};
@@ -192,6 +196,7 @@ struct Ctx {
     if (cap_s) cudaStreamDestroy(cap_s);
     for (void* p : allocs) cudaFree(p);
     if (feat_h) cudaFreeHost(feat_h);
+    if (err_h) cudaFreeHost(err_h);
     if (force_h) cudaFreeHost(force_h);
     for (auto& e : fev)
       if (e) cudaEventDestroy(e);
@@ -227,8 +232,8 @@ static void install_decomposition(Ctx& x, int which) {
     // at most 256 rows); used while the z-solver selects it
     if (x.mixed && x.nz - 2 <= 256) {
       auto bytes = [&x](size_t n) -> void* { return x.dalloc<unsigned char>(n); };
-      islice_build(x.opEinv[which].isl, Ei, x.nz, x.nz, 5, x.M, bytes);
-      islice_build(x.opE[which].isl, E, x.nz, x.nz, 5, x.M, bytes);
+      islice_build(x.opEinv[which].isl, Ei, x.nz, x.nz, 5, x.M, bytes, x.isl_err);
+      islice_build(x.opE[which].isl, E, x.nz, x.nz, 5, x.M, bytes, x.isl_err);
     }
   }
   x.opEinv[which].use_isl = x.opE[which].use_isl = x.zsolver == TG_ZSOLVER_ISLICE;
@@ -256,6 +261,7 @@ static Ctx* create(const tg_case& c) {
   x.mixed = c.precision == TG_PREC_MIXED;
   // mixed precision: the dense solves on the int8-slice tensor-core product
   x.zsolver = x.mixed ? TG_ZSOLVER_ISLICE : TG_ZSOLVER_DMMA;
+  x.isl_err = x.dalloc<int>(1);
   x.scalar = c.nphase > 1;
   x.opentop = std::fabs(c.bc_u[2] - 0) <= kSmall && std::fabs(c.bc_u[3] - 1) <= kSmall;  // boundary.cc:59-71
   x.dt = c.dt;
@@ -414,6 +420,8 @@ static Ctx* create(const tg_case& c) {
   x.bits = x.dalloc<unsigned long long>(16);
   TG_CUDA(cudaMallocHost(&x.feat_h, 2 * 100 * sizeof(double)));
   std::memset(x.feat_h, 0, 2 * 100 * sizeof(double));
+  TG_CUDA(cudaMallocHost(&x.err_h, 2 * sizeof(int)));
+  x.err_h[0] = x.err_h[1] = 0;
   x.force_d = x.dalloc<double>(2);
   TG_CUDA(cudaMallocHost(&x.force_h, 4 * sizeof(double)));
   std::memset(x.force_h, 0, 4 * sizeof(double));
@@ -1068,6 +1076,8 @@ static void enqueue_step(Ctx& x, int slot) {
   }
   x.alternation = !x.alternation;
   TG_CUDA(cudaMemcpyAsync(x.feat_h + slot * 100, x.feat, 100 * sizeof(double), cudaMemcpyDeviceToHost, x.s));
+  if (x.zsolver == TG_ZSOLVER_ISLICE)
+    TG_CUDA(cudaMemcpyAsync(x.err_h + slot, x.isl_err, sizeof(int), cudaMemcpyDeviceToHost, x.s));
   TG_CUDA(cudaEventRecord(x.fev[slot], x.s));
 }
 
@@ -1078,11 +1088,18 @@ struct StepLoop {
   double prev_f19 = 0.0;
 };
 
+// the int8-slice products of a step reported a bounded wait that gave up
+static void check_islice_flag(const Ctx& x, int slot) {
+  if (x.zsolver == TG_ZSOLVER_ISLICE && x.err_h[slot])
+    throw Error{TG_ERR_TIMEOUT, "FlatCarrierPhase::Helmholtz > a bounded wait of the int8-slice product gave up"};
+}
+
 static void check_step(Ctx& x, StepLoop& L, int maxstep, double maxcfl) {
   bool fwd_flag = x.step < maxstep;
   if (L.pending >= 0) {
     TG_CUDA(cudaEventSynchronize(x.fev[L.pending]));
     L.prev_f19 = x.feat_h[L.pending * 100 + 50 + 19];
+    check_islice_flag(x, L.pending);
   }
   x.cfl = L.prev_f19 * x.dt;
   if (!std::isfinite(L.prev_f19)) throw Error{TG_ERR_NAN, "TimeStepper::Update > non-finite CFL feature"};
@@ -1097,6 +1114,7 @@ static void finish_steps(Ctx& x, StepLoop& L, double* feat_out) {
   if (L.pending >= 0) {
     std::memcpy(x.feat_h + 100 * (L.pending ^ 1), x.feat_h + 100 * L.pending, 100 * sizeof(double));
     if (feat_out) std::memcpy(feat_out, x.feat_h + L.pending * 100 + 50, 50 * sizeof(double));
+    check_islice_flag(x, L.pending);
     if (!std::isfinite(x.feat_h[L.pending * 100 + 50 + 19]))
       throw Error{TG_ERR_NAN, "FlatCarrierPhase::Correct > non-finite velocity features"};
   }
@@ -1851,6 +1869,37 @@ tg_status tg_multiply_islice(tg_ctx* ctx, const double* A_host, const double* in
   });
 }
 
+tg_status tg_islice_selftest(tg_ctx* ctx) {
+  TG_CHECK_CTX(ctx);
+  Ctx& x = *reinterpret_cast<Ctx*>(ctx);
+  if (x.nz - 2 > 256) {
+    set_error("tg_islice_selftest > the int8-slice product needs nz <= 258");
+    return TG_ERR_SHAPE;
+  }
+  TG_TRY({
+    TG_CUDA(cudaStreamSynchronize(x.s));
+    // a product of the identity whose operator copies are withheld: its
+    // bounded wait for them gives up, the kernel drains, frees its tensor
+    // memory, sets the flag and returns
+    std::vector<double> A((size_t)x.nz * x.nz, 0.0);
+    for (int i = 0; i < x.nz; ++i) A[(size_t)i * x.nz + i] = 1.0;
+    auto bytes = [&x](size_t n) -> void* { return x.dalloc<unsigned char>(n); };
+    islice_build(x.islTmp, A, x.nz, x.nz, 5, x.M, bytes);
+    islice_clear_error(*x.islTmp);
+    EpiParams ep;
+    ep.nz = x.nz;
+    ep.M = x.M;
+    const IsliceOp* o = x.islTmp;
+    const double2* in = x.U;
+    double2* out = x.TMP;
+    islice_group(&o, &in, &out, &ep, 1, x.M, x.s, true);
+    TG_CUDA(cudaStreamSynchronize(x.s));
+    const int flag = islice_error(*x.islTmp);
+    islice_clear_error(*x.islTmp);
+    if (flag) throw Error{TG_ERR_TIMEOUT, "tg_islice_selftest > a bounded wait of the int8-slice product gave up"};
+  });
+}
+
 tg_status tg_set_zsolver(tg_ctx* ctx, int solver) {
   TG_CHECK_CTX(ctx);
   Ctx& x = *reinterpret_cast<Ctx*>(ctx);
@@ -1877,10 +1926,8 @@ tg_status tg_zsolver_error(tg_ctx* ctx, int* flag) {
   TG_TRY({
     TG_CUDA(cudaStreamSynchronize(x.s));
     int f = 0;
-    for (int i = 0; i < 5; ++i) {
-      if (x.opEinv[i].isl) f |= islice_error(*x.opEinv[i].isl);
-      if (x.opE[i].isl) f |= islice_error(*x.opE[i].isl);
-    }
+    TG_CUDA(cudaMemcpy(&f, x.isl_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (x.islTmp) f |= islice_error(*x.islTmp);
     *flag = f;
   });
 }

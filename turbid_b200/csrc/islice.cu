@@ -52,7 +52,11 @@ constexpr int BM = 128;                 // data columns per CTA (MMA M, tensor-m
 constexpr int kGemmThreads = 512;        // 16 warps: 4 per lane quarter of the accumulators
 constexpr int kTileX = BM * KP;         // bytes of one data tile
 constexpr int kBadExp = INT_MIN;        // column exponent of a column holding NaN or inf
-constexpr long long kSpin = 1ll << 22;  // polls of a bounded wait (each try_wait may suspend)
+// A bounded wait polls at most kSpin times, each poll suspending the thread
+// for at most kSuspendNs (a hint: it wakes as soon as the phase completes):
+// about one second in all, far beyond any wait of a working product.
+constexpr long long kSpin = 1ll << 20;
+constexpr uint32_t kSuspendNs = 1000;
 
 template <int S>
 struct IslShape {
@@ -109,10 +113,10 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
     uint32_t done = 0;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
         "selp.u32 %0, 1, 0, p;\n\t}"
         : "=r"(done)
-        : "r"(bar), "r"(parity)
+        : "r"(bar), "r"(parity), "n"(kSuspendNs)
         : "memory");
     if (done) return true;
   }
@@ -239,6 +243,7 @@ struct IslArgs {
   IslProblem p[kMaxIsl];   // blockIdx.y selects the problem
   int nz, nrow, ncol, ntiles, nchunks;
   int* err;
+  int withhold;            // failure-path check: the operator copies are never issued
 };
 
 // One CTA per 128 data columns, 16 warps.  Thread 0 issues the bulk copies
@@ -297,6 +302,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1) k_islice_gemm(const IslArgs a
   // exit can drain them
   int issued = 0;
   auto issue_op_load = [&](int it) {
+    if (args.withhold) return;   // failure-path check: the full-buffer wait will give up
     const int buf = it % NBUF;
     // iteration order = chunk-major, slice, K half: the half tiles lie in that order
     const int8_t* src = a.as + (size_t)it * kHalf;
@@ -511,7 +517,7 @@ static void slice_operator_host(const std::vector<double>& A, int nrow, int nz, 
 }
 
 void islice_build(IsliceOp*& op, const std::vector<double>& A, int nrow, int nz, int S, int M,
-                  const std::function<void*(size_t)>& alloc) {
+                  const std::function<void*(size_t)>& alloc, int* err) {
   if (S != 5) throw Error{TG_ERR_ARG, "islice > only 5 slices are built"};
   if (nz < 3 || nz - 2 > KP) throw Error{TG_ERR_SHAPE, "islice > nz - 2 must be at most 256"};
   if ((size_t)A.size() != (size_t)nrow * nz) throw Error{TG_ERR_SHAPE, "islice > operator size"};
@@ -539,8 +545,12 @@ void islice_build(IsliceOp*& op, const std::vector<double>& A, int nrow, int nz,
     o->aux = static_cast<double*>(alloc(aux.size() * sizeof(double)));
     o->xs = static_cast<int8_t*>(alloc((size_t)o->ntiles * S * kTileX));
     o->xe = static_cast<int*>(alloc((size_t)o->ntiles * BM * sizeof(int)));
-    o->err = static_cast<int*>(alloc(sizeof(int)));
-    TG_CUDA(cudaMemset(o->err, 0, sizeof(int)));
+    if (err) {
+      o->err = err;   // the caller's flag (shared by its products)
+    } else {
+      o->err = static_cast<int*>(alloc(sizeof(int)));
+      TG_CUDA(cudaMemset(o->err, 0, sizeof(int)));
+    }
     op = o.release();
   }
   TG_CUDA(cudaMemcpy(op->as, tiles.data(), tiles.size(), cudaMemcpyHostToDevice));
@@ -552,7 +562,7 @@ void islice_destroy(IsliceOp* op) { delete op; }   // device buffers belong to t
 // Problems of one group: each batch component of each problem is one problem of
 // the launch pair (slicing, then product), at most kMaxIsl per pair.
 void islice_group(const IsliceOp* const* ops, const double2* const* ins, double2* const* outs,
-                  const EpiParams* eps, int n, int M, cudaStream_t s) {
+                  const EpiParams* eps, int n, int M, cudaStream_t s, bool withhold_operator) {
   using Sh = IslShape<5>;
   if (n < 1 || n > kMaxIsl) throw Error{TG_ERR_ARG, "islice > bad group size"};
   const IsliceOp& op0 = *ops[0];
@@ -589,6 +599,7 @@ void islice_group(const IsliceOp* const* ops, const double2* const* ins, double2
   a.ntiles = op0.ntiles;
   a.nchunks = op0.nchunks;
   a.err = op0.err;
+  a.withhold = withhold_operator ? 1 : 0;
   const double by = n * (16.0 * M * op0.nz * 2 + (double)op0.ntiles * 5 * kTileX * 2);
   const double fl = n * 4.0 * op0.nz * op0.nz * (double)M;
   prof_begin(s, PC_ISLICE, by, fl, fl);
@@ -618,5 +629,6 @@ int islice_error(const IsliceOp& op) {
   TG_CUDA(cudaMemcpy(&v, op.err, sizeof(int), cudaMemcpyDeviceToHost));
   return v;
 }
+void islice_clear_error(const IsliceOp& op) { TG_CUDA(cudaMemset(op.err, 0, sizeof(int))); }
 
 }  // namespace tg

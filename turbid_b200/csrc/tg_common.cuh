@@ -203,15 +203,16 @@ struct IsliceOp;
 // components of M modes; op is built on the first call and refilled (same
 // shape) on later ones.  Device memory through alloc (owned by the caller).
 void islice_build(IsliceOp*& op, const std::vector<double>& A, int nrow, int nz, int S, int M,
-                  const std::function<void*(size_t)>& alloc);
+                  const std::function<void*(size_t)>& alloc, int* err = nullptr);
 void islice_destroy(IsliceOp* op);
 // n <= 3 problems (distinct operators), one launch pair: out_i = epi_i(A_i in_i)
 void islice_group(const IsliceOp* const* ops, const double2* const* ins, double2* const* outs,
-                  const EpiParams* eps, int n, int M, cudaStream_t s);
+                  const EpiParams* eps, int n, int M, cudaStream_t s, bool withhold_operator = false);
 void islice_apply(const IsliceOp& op, const double2* in, long long in_stride, double2* out, long long out_stride,
                   int M, int batch, const EpiParams& ep, cudaStream_t s);
-// the error flag of the product's bounded waits (synchronous read)
+// the error flag of the product's bounded waits (synchronous read, clear)
 int islice_error(const IsliceOp& op);
+void islice_clear_error(const IsliceOp& op);
 
 // A real nz x nz operator resident on the device: the dense copy and, when
 // it is centro-symmetric (sgn +1) or centro-antisymmetric (sgn -1), the two
