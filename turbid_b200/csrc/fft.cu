@@ -422,45 +422,92 @@ __global__ void __launch_bounds__(NB * L / 16) fx_p2_kernel(TransformDims d, con
   } else {
     src = phys + (size_t)plane * d.ny * L;
   }
-  {
-    constexpr int IT = NB * L / (NT * VW);  // every load of the tile in flight before the first shared store
-    R va[IT], vb[IT];
-    R wa[PROD ? IT : 1], wb[PROD ? IT : 1];
+  if constexpr (L >= 16) {
+    {
+      // the first radix-16 pass straight from the rows: thread (b, j) takes the
+      // 16 values x = j + r * L/16 of row pair b (for each r the threads of a
+      // row pair read 16 consecutive reals), so the tile is not staged in
+      // shared memory before the pass; one butterfly per thread (NT = NB * L/16)
+      constexpr int nb = L / 16;
+      const int b = threadIdx.x / nb, j = threadIdx.x - b * nb;
+      const int ya = y0 + 2 * b, yb = ya + 1;
+      const bool oka = ya < d.ny, okb = yb < d.ny;
+      const T* ra = src + (size_t)(oka ? ya : 0) * L + j;
+      const T* rb = src + (size_t)(okb ? yb : 0) * L + j;
+      T va[16], vb[16];
 #pragma unroll
-    for (int i = 0; i < IT; ++i) {
-      const int e = (threadIdx.x + i * NT) * VW;
-      const int p = e / L, x = e % L;
-      const int ya = y0 + 2 * p, yb = ya + 1;
-      va[i] = ya < d.ny ? *reinterpret_cast<const R*>(src + (size_t)ya * L + x) : vzero<R>();
-      vb[i] = yb < d.ny ? *reinterpret_cast<const R*>(src + (size_t)yb * L + x) : vzero<R>();
+      for (int r = 0; r < 16; ++r) {   // every load in flight before the first use
+        va[r] = oka ? ra[r * nb] : T(0);
+        vb[r] = okb ? rb[r * nb] : T(0);
+      }
       if constexpr (PROD) {
-        if (srcb) {
-          wa[i] = ya < d.ny ? *reinterpret_cast<const R*>(srcb + (size_t)ya * L + x) : vzero<R>();
-          wb[i] = yb < d.ny ? *reinterpret_cast<const R*>(srcb + (size_t)yb * L + x) : vzero<R>();
+        if (srcb) {  // a * (b + shift), the products of the reference's physical-space step
+          const T* wa = srcb + (size_t)(oka ? ya : 0) * L + j;
+          const T* wb = srcb + (size_t)(okb ? yb : 0) * L + j;
+          T xa[16], xb[16];
+#pragma unroll
+          for (int r = 0; r < 16; ++r) {
+            xa[r] = oka ? wa[r * nb] : T(0);
+            xb[r] = okb ? wb[r * nb] : T(0);
+          }
+#pragma unroll
+          for (int r = 0; r < 16; ++r) {
+            va[r] = va[r] * (xa[r] + shb);
+            vb[r] = vb[r] * (xb[r] + shb);
+          }
         }
       }
+      C v[16];
+#pragma unroll
+      for (int r = 0; r < 16; ++r) v[r] = mkc<C>(va[r], vb[r]);
+      dft_ct<16, -1>(v);
+      C* row = buf + b * RS;
+#pragma unroll
+      for (int k = 0; k < 16; ++k) row[sp(16 * j + k)] = v[k];
     }
-    if constexpr (PROD) {
-      if (srcb) {  // a * (b + shift), the products of the reference's physical-space step
+    __syncthreads();
+    ip_passes<T, -1, L, NB, 16>(buf, tw);
+  } else {  // L = 8: one radix-8 pass, two butterflies a thread
+    {
+      constexpr int IT = NB * L / (NT * VW);  // every load of the tile in flight before the first shared store
+      R va[IT], vb[IT];
+      R wa[PROD ? IT : 1], wb[PROD ? IT : 1];
 #pragma unroll
-        for (int i = 0; i < IT; ++i)
-#pragma unroll
-          for (int j = 0; j < VW; ++j) {
-            vset(va[i], j, vget(va[i], j) * (vget(wa[i], j) + shb));
-            vset(vb[i], j, vget(vb[i], j) * (vget(wb[i], j) + shb));
+      for (int i = 0; i < IT; ++i) {
+        const int e = (threadIdx.x + i * NT) * VW;
+        const int p = e / L, x = e % L;
+        const int ya = y0 + 2 * p, yb = ya + 1;
+        va[i] = ya < d.ny ? *reinterpret_cast<const R*>(src + (size_t)ya * L + x) : vzero<R>();
+        vb[i] = yb < d.ny ? *reinterpret_cast<const R*>(src + (size_t)yb * L + x) : vzero<R>();
+        if constexpr (PROD) {
+          if (srcb) {
+            wa[i] = ya < d.ny ? *reinterpret_cast<const R*>(srcb + (size_t)ya * L + x) : vzero<R>();
+            wb[i] = yb < d.ny ? *reinterpret_cast<const R*>(srcb + (size_t)yb * L + x) : vzero<R>();
           }
+        }
+      }
+      if constexpr (PROD) {
+        if (srcb) {  // a * (b + shift), the products of the reference's physical-space step
+#pragma unroll
+          for (int i = 0; i < IT; ++i)
+#pragma unroll
+            for (int j = 0; j < VW; ++j) {
+              vset(va[i], j, vget(va[i], j) * (vget(wa[i], j) + shb));
+              vset(vb[i], j, vget(vb[i], j) * (vget(wb[i], j) + shb));
+            }
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < IT; ++i) {
+        const int e = (threadIdx.x + i * NT) * VW;
+        const int p = e / L, x = e % L;
+#pragma unroll
+        for (int j = 0; j < VW; ++j) buf[p * RS + sp(x + j)] = mkc<C>(vget(va[i], j), vget(vb[i], j));
       }
     }
-#pragma unroll
-    for (int i = 0; i < IT; ++i) {
-      const int e = (threadIdx.x + i * NT) * VW;
-      const int p = e / L, x = e % L;
-#pragma unroll
-      for (int j = 0; j < VW; ++j) buf[p * RS + sp(x + j)] = mkc<C>(vget(va[i], j), vget(vb[i], j));
-    }
+    __syncthreads();
+    ip_passes<T, -1, L, NB, 1>(buf, tw);
   }
-  __syncthreads();
-  ip_passes<T, -1, L, NB, 1>(buf, tw);
   C* dst = work + (size_t)plane * d.nxh * d.ny;
   for (int idx = threadIdx.x; idx < rows * d.nxh; idx += NT) {
     const int k = idx / rows, q = idx % rows;
@@ -693,23 +740,34 @@ __global__ void __launch_bounds__(NB * L / 16) bx_p2_kernel(TransformDims d, con
   const int y0 = blockIdx.x * rows;
   bx_fill<T, L, NB>(buf, d, work, plane, y0);
   __syncthreads();
-  ip_passes<T, +1, L, NB, 1>(buf, tw);
   T* dst = phys + (size_t)plane * d.ny * L;
-  constexpr int IS = NB * L / (NT * VW);
+  if constexpr (L >= 16) {
+    // the last pass writes the rows itself (threads of a row pair store
+    // consecutive x), so its outputs are not staged in shared memory
+    ip_passes<T, +1, L, NB, 1, NT, last_stride(L)>(buf, tw);
+    last_pass_out<T, +1, L, NB, NT>(buf, tw, [&](int p, int x, int, C z) {
+      const int ya = y0 + 2 * p, yb = ya + 1;
+      if (ya < d.ny) dst[(size_t)ya * L + x] = z.x;
+      if (yb < d.ny) dst[(size_t)yb * L + x] = z.y;
+    });
+  } else {
+    ip_passes<T, +1, L, NB, 1>(buf, tw);
+    constexpr int IS = NB * L / (NT * VW);
 #pragma unroll 4
-  for (int i = 0; i < IS; ++i) {
-    const int e = (threadIdx.x + i * NT) * VW;
-    const int p = e / L, x = e % L;
-    const int ya = y0 + 2 * p, yb = ya + 1;
-    R ra, rb;
+    for (int i = 0; i < IS; ++i) {
+      const int e = (threadIdx.x + i * NT) * VW;
+      const int p = e / L, x = e % L;
+      const int ya = y0 + 2 * p, yb = ya + 1;
+      R ra, rb;
 #pragma unroll
-    for (int j = 0; j < VW; ++j) {
-      const C z = buf[p * RS + sp(x + j)];
-      vset(ra, j, z.x);
-      vset(rb, j, z.y);
+      for (int j = 0; j < VW; ++j) {
+        const C z = buf[p * RS + sp(x + j)];
+        vset(ra, j, z.x);
+        vset(rb, j, z.y);
+      }
+      if (ya < d.ny) *reinterpret_cast<R*>(dst + (size_t)ya * L + x) = ra;
+      if (yb < d.ny) *reinterpret_cast<R*>(dst + (size_t)yb * L + x) = rb;
     }
-    if (ya < d.ny) *reinterpret_cast<R*>(dst + (size_t)ya * L + x) = ra;
-    if (yb < d.ny) *reinterpret_cast<R*>(dst + (size_t)yb * L + x) = rb;
   }
 }
 

@@ -100,10 +100,11 @@ template <int L> struct P2 {
   static constexpr int RS = L + L / 16 + 1;  // padded row stride (complex values)
 };
 
-template <typename T, int DIR, int L, int NB, int Ns, int NT = NB * L / 16>
+// the passes of strides Ns, Ns * 16, ... below NsEnd (all remaining ones by default)
+template <typename T, int DIR, int L, int NB, int Ns, int NT = NB * L / 16, int NsEnd = L>
 __device__ __forceinline__ void ip_passes(cplx<T>* buf, const cplx<T>* __restrict__ tw, int tid = threadIdx.x) {
   using C = cplx<T>;
-  if constexpr (Ns < L) {
+  if constexpr (Ns < L && Ns < NsEnd) {
     constexpr int rem = L / Ns;
     constexpr int R = rem >= 16 ? 16 : rem;
     constexpr int nb = L / R;                    // butterflies per transform
@@ -142,7 +143,51 @@ __device__ __forceinline__ void ip_passes(cplx<T>* buf, const cplx<T>* __restric
       }
     }
     __syncthreads();
-    ip_passes<T, DIR, L, NB, Ns * R, NT>(buf, tw, tid);
+    ip_passes<T, DIR, L, NB, Ns * R, NT, NsEnd>(buf, tw, tid);
+  }
+}
+
+// stride of the last pass of a length-L transform (passes of radix 16, the
+// last one of radix L / stride)
+__host__ __device__ constexpr int last_stride(int L) {
+  int ns = 1;
+  while (ns * 16 < L) ns *= 16;
+  return ns;
+}
+
+// The last pass (stride Ns = last_stride(L)) reading the padded rows and
+// handing each output, with its transform b, index x and slot i in the
+// thread (0 .. NB*L/NT - 1, a compile-time constant once unrolled), to
+// out(b, x, i, value) instead of writing it back: used where the pass's
+// outputs leave for global memory.  Call after the earlier passes and a
+// barrier.
+template <typename T, int DIR, int L, int NB, int NT, typename Out>
+__device__ __forceinline__ void last_pass_out(const cplx<T>* buf, const cplx<T>* __restrict__ tw, Out&& out,
+                                              int tid = threadIdx.x) {
+  using C = cplx<T>;
+  constexpr int Ns = last_stride(L);
+  constexpr int R = L / Ns;
+  constexpr int nb = L / R;                    // = Ns
+  constexpr int groups = NB * nb;
+  constexpr int GPT = (groups + NT - 1) / NT;
+  constexpr bool exact = groups % NT == 0;
+  constexpr int RS = P2<L>::RS;
+#pragma unroll
+  for (int t = 0; t < GPT; ++t) {
+    const int g = tid + t * NT;
+    if (exact || g < groups) {
+      const int b = g / nb, j = g - b * nb;   // j < Ns: the twiddle index and the output base
+      const C* src = buf + b * RS;
+      C v[R];
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        v[r] = src[sp(j + r * nb)];
+        if (Ns > 1 && r > 0) v[r] = cmul(v[r], tw_get<T, DIR>(tw, j * r));
+      }
+      dft_ct<R, DIR>(v);
+#pragma unroll
+      for (int k = 0; k < R; ++k) out(b, j + k * Ns, t * R + k, v[k]);
+    }
   }
 }
 
