@@ -620,9 +620,17 @@ static void carrier_predict(Ctx& x, int stage) {
   }
   if (x.scalar && x.c.scalar_bc == 1) {
     // bottom plane of du/dz, dv/dz in physical space for the erosion flux
-    const size_t pl = (size_t)x.nx * x.ny;
-    bwd<T>(x, x.DU + 2 * S, (T*)x.PLN, 1);
-    bwd<T>(x, x.DU + 5 * S, (T*)x.PLN + pl, 1);
+    // (one gathered transform of the two planes: the gather takes plane f of
+    // its sources as field f when the dimensions say one plane per field)
+    SpecGather g{};
+    g.src[0] = x.DU + 2 * S;
+    g.src[1] = x.DU + 5 * S;
+    g.kx = x.kx;
+    g.ky = x.ky;
+    g.nf = 2;
+    TransformDims d1 = x.td;
+    d1.nz = 1;
+    dft_backward<T>(d1, x.px, x.py, nullptr, (T*)x.PLN, 2, x.work, x.s, &g);
   }
   // H = c1 H - dt adv; buoyancy; mean-mode force
   double bcoef = 0.0;
