@@ -738,9 +738,45 @@ __global__ void __launch_bounds__(NB * L / 16) bx_p2_kernel(TransformDims d, con
   C* buf = reinterpret_cast<C*>(smem_raw);
   const int plane = blockIdx.y;
   const int y0 = blockIdx.x * rows;
+  T* dst = phys + (size_t)plane * d.ny * L;
+  if constexpr (L >= 32 && PV::kBwdRowMajor) {
+    // the first radix-16 pass straight from the spectral rows: thread (b, j)
+    // forms Z[x] = X1[x] + i X2[x] of row pair b at x = j + r * L/16 (X[L-k]
+    // = conj X[k]; zero between the kept bands), so the packed rows are not
+    // staged in shared memory before the pass
+    constexpr int nb = L / 16, nxh = L / 3 * 2 / 2 + 1;
+    const int b = threadIdx.x / nb, j = threadIdx.x - b * nb;
+    const int ya = y0 + 2 * b, yb = ya + 1;
+    const bool oka = ya < d.ny, okb = yb < d.ny;
+    const C* src = work + (size_t)plane * nxh * d.ny;
+    const C* r1 = src + (size_t)(oka ? ya : 0) * nxh;
+    const C* r2 = src + (size_t)(okb ? yb : 0) * nxh;
+    C v[16];
+#pragma unroll
+    for (int r = 0; r < 16; ++r) {
+      const int x = j + r * nb;
+      const bool lo = x < nxh, hi = x > L - nxh;
+      const int k = lo ? x : L - x;
+      C a = (oka && (lo || hi)) ? r1[k] : mkc<C>(0, 0);
+      C c = (okb && (lo || hi)) ? r2[k] : mkc<C>(0, 0);
+      if (x == 0) a.y = c.y = T(0);
+      v[r] = lo ? mkc<C>(a.x - c.y, a.y + c.x) : mkc<C>(a.x + c.y, -a.y + c.x);
+    }
+    dft_ct<16, +1>(v);
+    C* row = buf + b * RS;
+#pragma unroll
+    for (int k = 0; k < 16; ++k) row[sp(16 * j + k)] = v[k];
+    __syncthreads();
+    ip_passes<T, +1, L, NB, 16, NT, last_stride(L)>(buf, tw);
+    last_pass_out<T, +1, L, NB, NT>(buf, tw, [&](int p, int x, int, C z) {
+      const int ra = y0 + 2 * p, rb = ra + 1;
+      if (ra < d.ny) dst[(size_t)ra * L + x] = z.x;
+      if (rb < d.ny) dst[(size_t)rb * L + x] = z.y;
+    });
+    return;
+  }
   bx_fill<T, L, NB>(buf, d, work, plane, y0);
   __syncthreads();
-  T* dst = phys + (size_t)plane * d.ny * L;
   if constexpr (L >= 16) {
     // the last pass writes the rows itself (threads of a row pair store
     // consecutive x), so its outputs are not staged in shared memory
