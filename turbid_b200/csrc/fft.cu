@@ -541,6 +541,35 @@ __global__ void __launch_bounds__(NB * L / 16) fy_p2_kernel(TransformDims d, con
   const int plane = blockIdx.y;
   const int k0 = blockIdx.x * NB;
   const C* src = work + (size_t)plane * d.nxh * L;
+  constexpr int nyc = L / 3 * 2;   // d.nyc of a power-of-two Ny = L
+  if constexpr (L >= 32) {
+    // the first radix-16 pass straight from the columns (thread (c, j) takes
+    // y = j + r * L/16 of column c) and the last one writing the kept modes
+    // itself: the column is staged in shared memory only between the two
+    constexpr int nb = L / 16;
+    const int c = threadIdx.x / nb, j = threadIdx.x - c * nb;
+    const bool okc = k0 + c < d.nxh;
+    const C* col = src + (size_t)(okc ? k0 + c : 0) * L + j;
+    C v[16];
+#pragma unroll
+    for (int r = 0; r < 16; ++r) v[r] = okc ? col[r * nb] : mkc<C>(0, 0);
+    dft_ct<16, -1>(v);
+    C* row = buf + c * RS;
+#pragma unroll
+    for (int k = 0; k < 16; ++k) row[sp(16 * j + k)] = v[k];
+    __syncthreads();
+    ip_passes<T, -1, L, NB, 16, NT, last_stride(L)>(buf, tw);
+    double2* dst = spec + (size_t)plane * d.M;
+    last_pass_out<T, -1, L, NB, NT>(buf, tw, [&](int cc, int y, int, C z) {
+      const int k = k0 + cc;
+      const bool lo = y < nyc / 2, hi = y >= L - nyc / 2;   // kept spectral rows
+      if (k < d.nxh && (lo || hi)) {
+        const int iy = lo ? y : y - (L - nyc);
+        dst[iy + (size_t)nyc * k] = make_double2((double)z.x * scale, (double)z.y * scale);
+      }
+    });
+    return;
+  }
   {
     constexpr int IT = NB * L / (NT * VC);
     CV v[IT];
@@ -561,7 +590,6 @@ __global__ void __launch_bounds__(NB * L / 16) fy_p2_kernel(TransformDims d, con
   __syncthreads();
   ip_passes<T, -1, L, NB, 1>(buf, tw);
   double2* dst = spec + (size_t)plane * d.M;
-  constexpr int nyc = L / 3 * 2;   // d.nyc of a power-of-two Ny = L
   for (int idx = threadIdx.x; idx < NB * nyc; idx += NT) {
     const int c = idx / nyc, iy = idx - c * nyc;
     const int k = k0 + c;
