@@ -679,6 +679,42 @@ __global__ void __launch_bounds__(NB * L / 16) by_p2_kernel(TransformDims d, con
 }
 
 // backward x pass, L = nx: two rows per complex FFT; Im of the kx = 0 coefficient ignored (c2r).
+// Backward x pass, first radix-16 pass straight from the row-major work
+// plane (FP32 layout [plane][y][kx], L >= 16): thread (b, j) forms Z[x] =
+// X1[x] + i X2[x] of row pair b at x = j + r * L/16 (X[L-k] = conj X[k]; zero
+// between the kept bands; Im of kx = 0 ignored), transforms the 16 values and
+// stores the pass's outputs in buf, so the packed rows are never staged in
+// shared memory before the pass.  One butterfly per thread (NB * L/16
+// threads); the caller synchronises and runs the passes of stride 16 on.
+template <typename T, int L, int NB>
+__device__ __forceinline__ void bx_first_pass(cplx<T>* buf, const TransformDims& d,
+                                              const cplx<T>* __restrict__ work, int plane, int y0) {
+  using C = cplx<T>;
+  constexpr int RS = P2<L>::RS;
+  constexpr int nb = L / 16, nxh = L / 3 * 2 / 2 + 1;
+  const int b = threadIdx.x / nb, j = threadIdx.x - b * nb;
+  const int ya = y0 + 2 * b, yb = ya + 1;
+  const bool oka = ya < d.ny, okb = yb < d.ny;
+  const C* src = work + (size_t)plane * nxh * d.ny;
+  const C* r1 = src + (size_t)(oka ? ya : 0) * nxh;
+  const C* r2 = src + (size_t)(okb ? yb : 0) * nxh;
+  C v[16];
+#pragma unroll
+  for (int r = 0; r < 16; ++r) {
+    const int x = j + r * nb;
+    const bool lo = x < nxh, hi = x > L - nxh;
+    const int k = lo ? x : L - x;
+    C a = (oka && (lo || hi)) ? r1[k] : mkc<C>(0, 0);
+    C c = (okb && (lo || hi)) ? r2[k] : mkc<C>(0, 0);
+    if (x == 0) a.y = c.y = T(0);
+    v[r] = lo ? mkc<C>(a.x - c.y, a.y + c.x) : mkc<C>(a.x + c.y, -a.y + c.x);
+  }
+  dft_ct<16, +1>(v);
+  C* row = buf + b * RS;
+#pragma unroll
+  for (int k = 0; k < 16; ++k) row[sp(16 * j + k)] = v[k];
+}
+
 // Backward x pass, loading half: the zero gap and the row pairs of one work
 // plane combined into the packed two-row FFT input in buf (shared memory).
 template <typename T, int L, int NB>
@@ -768,32 +804,7 @@ __global__ void __launch_bounds__(NB * L / 16) bx_p2_kernel(TransformDims d, con
   const int y0 = blockIdx.x * rows;
   T* dst = phys + (size_t)plane * d.ny * L;
   if constexpr (L >= 32 && PV::kBwdRowMajor) {
-    // the first radix-16 pass straight from the spectral rows: thread (b, j)
-    // forms Z[x] = X1[x] + i X2[x] of row pair b at x = j + r * L/16 (X[L-k]
-    // = conj X[k]; zero between the kept bands), so the packed rows are not
-    // staged in shared memory before the pass
-    constexpr int nb = L / 16, nxh = L / 3 * 2 / 2 + 1;
-    const int b = threadIdx.x / nb, j = threadIdx.x - b * nb;
-    const int ya = y0 + 2 * b, yb = ya + 1;
-    const bool oka = ya < d.ny, okb = yb < d.ny;
-    const C* src = work + (size_t)plane * nxh * d.ny;
-    const C* r1 = src + (size_t)(oka ? ya : 0) * nxh;
-    const C* r2 = src + (size_t)(okb ? yb : 0) * nxh;
-    C v[16];
-#pragma unroll
-    for (int r = 0; r < 16; ++r) {
-      const int x = j + r * nb;
-      const bool lo = x < nxh, hi = x > L - nxh;
-      const int k = lo ? x : L - x;
-      C a = (oka && (lo || hi)) ? r1[k] : mkc<C>(0, 0);
-      C c = (okb && (lo || hi)) ? r2[k] : mkc<C>(0, 0);
-      if (x == 0) a.y = c.y = T(0);
-      v[r] = lo ? mkc<C>(a.x - c.y, a.y + c.x) : mkc<C>(a.x + c.y, -a.y + c.x);
-    }
-    dft_ct<16, +1>(v);
-    C* row = buf + b * RS;
-#pragma unroll
-    for (int k = 0; k < 16; ++k) row[sp(16 * j + k)] = v[k];
+    bx_first_pass<T, L, NB>(buf, d, work, plane, y0);
     __syncthreads();
     ip_passes<T, +1, L, NB, 16, NT, last_stride(L)>(buf, tw);
     last_pass_out<T, +1, L, NB, NT>(buf, tw, [&](int p, int x, int, C z) {
@@ -865,9 +876,15 @@ __global__ void __launch_bounds__(NB * L / 16, sizeof(T) == 4 ? 640 / (NB * L / 
 #pragma unroll 1
   for (int j = 0; j < 3; ++j) {
     if (j > 0) __syncthreads();   // buf is refilled
-    bx_fill<T, L, NB>(buf, d, work, (3 * c + j) * d.nz + z, y0);
-    __syncthreads();
-    ip_passes<T, +1, L, NB, 1>(buf, tw);
+    if constexpr (L >= 16 && PV::kBwdRowMajor) {
+      bx_first_pass<T, L, NB>(buf, d, work, (3 * c + j) * d.nz + z, y0);
+      __syncthreads();
+      ip_passes<T, +1, L, NB, 16>(buf, tw);
+    } else {
+      bx_fill<T, L, NB>(buf, d, work, (3 * c + j) * d.nz + z, y0);
+      __syncthreads();
+      ip_passes<T, +1, L, NB, 1>(buf, tw);
+    }
     const T* uj = unl + (size_t)j * P + zoff;
     const T sh = (T)(j == 0 ? su : j == 1 ? sv : sw);
 #pragma unroll
