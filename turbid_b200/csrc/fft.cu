@@ -364,11 +364,13 @@ __global__ void __launch_bounds__(256) bwd_x_kernel(TransformDims d, PlanArgs pl
   }
 }
 
-// Per-precision access widths of the p2 kernels.  FP32: 16-byte vectors (four
-// reals of a row, two complex values of a column) and the backward
-// intermediate row-major [plane][y][kx], so that the backward x pass reads
-// contiguous row blocks.  FP64: one real / one complex value per access and
-// the backward intermediate [plane][kx][y] (measured faster for 16-byte
+// Per-precision access widths of the p2 kernels' staged paths (the lengths
+// below 16 or 32 and the FP64 backward x pass; longer rows and columns form
+// their first radix-16 butterfly from per-thread loads).  FP32: 16-byte
+// vectors (four reals of a row, two complex values of a column) and the
+// backward intermediate row-major [plane][y][kx], so that the backward x pass
+// reads contiguous row blocks.  FP64: one real / one complex value per access
+// and the backward intermediate [plane][kx][y] (measured faster for 16-byte
 // complex values, whose accesses are already wide).
 template <typename T> struct P2Vec;
 template <> struct P2Vec<float> {
