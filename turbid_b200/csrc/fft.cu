@@ -614,54 +614,83 @@ __global__ void __launch_bounds__(NB * L / 16) by_p2_kernel(TransformDims d, con
   const int plane = blockIdx.y;
   const int k0 = blockIdx.x * NB;
   constexpr int nyc = L / 3 * 2;   // d.nyc of a power-of-two Ny = L
-  constexpr int gap = L - nyc;  // FFT indices [nyc/2, L - nyc/2) carry no spectral row
-  for (int idx = threadIdx.x; idx < NB * gap; idx += NT) {
-    const int c = idx / gap, y = nyc / 2 + (idx - c * gap);
-    buf[c * RS + sp(y)] = mkc<C>(0, 0);
-  }
   int deriv = 0;
   const double2* src = GATHER ? gather_src(gat, plane, d.nz, d.M, deriv) : spec + (size_t)plane * d.M;
-  if constexpr (RM) {
-    // the NB columns are one contiguous run of NB*nyc coefficients; every
-    // load in flight before the first shared store
-    constexpr int IT = (NB * (L / 3 * 2) + NT - 1) / NT;  // nyc = L/3*2
-    const int run = min(NB, d.nxh - k0) * nyc;
-    const double2* s0 = src + (size_t)k0 * nyc;
-    double2 v[IT];
-    double kf[GATHER ? IT : 1];   // wavenumber of a derivative, loaded with the coefficient
+  if constexpr (L >= 16 && !GATHER) {
+    // the first radix-16 pass straight from the spectral columns: thread
+    // (c, j) takes y = j + r * L/16 of column c (zero between the kept
+    // bands), so the column is not staged in shared memory before the pass.
+    // (The gathered form keeps the staged load: its derivative factors made
+    // the per-thread loads slower than the one contiguous run.)
+    constexpr int nb = L / 16;
+    const int c = threadIdx.x / nb, j = threadIdx.x - c * nb;
+    const int k = k0 + c;
+    const bool okc = k < d.nxh;
+    const double2* col = src + (size_t)(okc ? k : 0) * nyc;
+    C v[16];
 #pragma unroll
-    for (int i = 0; i < IT; ++i) {
-      const int idx = threadIdx.x + i * NT;
-      v[i] = idx < run ? s0[idx] : make_double2(0.0, 0.0);
-      if constexpr (GATHER) {
-        const double* kt = deriv == 1 ? gat.kx : gat.ky;
-        kf[i] = (deriv != 0 && idx < run) ? kt[k0 * nyc + idx] : 0.0;
-      }
+    for (int r = 0; r < 16; ++r) {
+      const int y = j + r * nb;
+      const bool lo = y < nyc / 2, hi = y >= L - nyc / 2;
+      const int iy = lo ? y : y - (L - nyc);
+      const bool ok = okc && (lo || hi);
+      double2 w = ok ? col[iy] : make_double2(0.0, 0.0);
+      v[r] = mkc<C>((T)w.x, (T)w.y);
     }
+    dft_ct<16, +1>(v);
+    C* row = buf + c * RS;
 #pragma unroll
-    for (int i = 0; i < IT; ++i) {
-      const int idx = threadIdx.x + i * NT;
-      if (idx < NB * nyc) {
-        const int c = idx / nyc, iy = idx - c * nyc;
-        double2 w = v[i];
-        if constexpr (GATHER) {
-          if (deriv != 0) w = make_double2(0.0 * v[i].x - kf[i] * v[i].y, 0.0 * v[i].y + kf[i] * v[i].x);
-        }
-        buf[c * RS + sp(y_of(iy, L, nyc))] = mkc<C>((T)w.x, (T)w.y);
-      }
-    }
+    for (int q = 0; q < 16; ++q) row[sp(16 * j + q)] = v[q];
+    __syncthreads();
+    ip_passes<T, +1, L, NB, 16>(buf, tw);
   } else {
-#pragma unroll 4
-    for (int idx = threadIdx.x; idx < NB * nyc; idx += NT) {
-      const int c = idx / nyc, iy = idx - c * nyc;
-      const int k = k0 + c;
-      const int m = iy + nyc * k;
-      double2 v = k < d.nxh ? (GATHER ? gather_value(gat, deriv, m, src[m]) : src[m]) : make_double2(0.0, 0.0);
-      buf[c * RS + sp(y_of(iy, L, nyc))] = mkc<C>((T)v.x, (T)v.y);
+    constexpr int gap = L - nyc;  // FFT indices [nyc/2, L - nyc/2) carry no spectral row
+    for (int idx = threadIdx.x; idx < NB * gap; idx += NT) {
+      const int c = idx / gap, y = nyc / 2 + (idx - c * gap);
+      buf[c * RS + sp(y)] = mkc<C>(0, 0);
     }
+    if constexpr (RM) {
+      // the NB columns are one contiguous run of NB*nyc coefficients; every
+      // load in flight before the first shared store
+      constexpr int IT = (NB * (L / 3 * 2) + NT - 1) / NT;  // nyc = L/3*2
+      const int run = min(NB, d.nxh - k0) * nyc;
+      const double2* s0 = src + (size_t)k0 * nyc;
+      double2 v[IT];
+      double kf[GATHER ? IT : 1];   // wavenumber of a derivative, loaded with the coefficient
+#pragma unroll
+      for (int i = 0; i < IT; ++i) {
+        const int idx = threadIdx.x + i * NT;
+        v[i] = idx < run ? s0[idx] : make_double2(0.0, 0.0);
+        if constexpr (GATHER) {
+          const double* kt = deriv == 1 ? gat.kx : gat.ky;
+          kf[i] = (deriv != 0 && idx < run) ? kt[k0 * nyc + idx] : 0.0;
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < IT; ++i) {
+        const int idx = threadIdx.x + i * NT;
+        if (idx < NB * nyc) {
+          const int c = idx / nyc, iy = idx - c * nyc;
+          double2 w = v[i];
+          if constexpr (GATHER) {
+            if (deriv != 0) w = make_double2(0.0 * v[i].x - kf[i] * v[i].y, 0.0 * v[i].y + kf[i] * v[i].x);
+          }
+          buf[c * RS + sp(y_of(iy, L, nyc))] = mkc<C>((T)w.x, (T)w.y);
+        }
+      }
+    } else {
+#pragma unroll 4
+      for (int idx = threadIdx.x; idx < NB * nyc; idx += NT) {
+        const int c = idx / nyc, iy = idx - c * nyc;
+        const int k = k0 + c;
+        const int m = iy + nyc * k;
+        double2 v = k < d.nxh ? (GATHER ? gather_value(gat, deriv, m, src[m]) : src[m]) : make_double2(0.0, 0.0);
+        buf[c * RS + sp(y_of(iy, L, nyc))] = mkc<C>((T)v.x, (T)v.y);
+      }
+    }
+    __syncthreads();
+    ip_passes<T, +1, L, NB, 1>(buf, tw);
   }
-  __syncthreads();
-  ip_passes<T, +1, L, NB, 1>(buf, tw);
   C* dst = work + (size_t)plane * d.nxh * L;
   if constexpr (RM) {
     // [plane][y][kx]: rows of NB kx values
