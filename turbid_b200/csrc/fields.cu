@@ -558,7 +558,10 @@ __global__ void k_feature_max(const T* __restrict__ unl, int nx, int ny, int nz,
   // blockIdx.y = z plane: the wall maxima and 1/glz need no per-element index division
   const size_t plane = (size_t)nx * ny, P = plane * nz;
   const int z = blockIdx.y;
-  const double gl = glz[z];
+  // the CFL length |u|/dx + |v|/dy + |w|/dz with the reciprocals taken once
+  // (three FP64 divisions per point were most of this kernel's time; the
+  // products differ from the quotients in the last bits only)
+  const double ilx = 1.0 / lmx, ily = 1.0 / lmy, igl = 1.0 / glz[z];
   const T* pu = unl + (size_t)z * plane;
   double mu = 0, mv = 0, mw = 0, ml = 0;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < plane; i += (size_t)gridDim.x * blockDim.x) {
@@ -566,7 +569,7 @@ __global__ void k_feature_max(const T* __restrict__ unl, int nx, int ny, int nz,
     mu = max_keep_nan(mu, u);
     mv = max_keep_nan(mv, v);
     mw = max_keep_nan(mw, w);
-    ml = max_keep_nan(ml, u / lmx + v / lmy + w / gl);
+    ml = max_keep_nan(ml, u * ilx + v * ily + w * igl);
   }
   double mx[4] = {mu, mv, mw, ml};
 #pragma unroll
