@@ -1,6 +1,8 @@
 // Elementwise stage kernels and reductions of the RK3 substep.
 // Each kernel restates one block of the reference's Armadillo expressions
 // (file:line cited per kernel), evaluated per element in the same order.
+#include <type_traits>
+
 #include "fields.cuh"
 
 namespace tg {
@@ -564,13 +566,29 @@ __global__ void k_feature_max(const T* __restrict__ unl, int nx, int ny, int nz,
   const double ilx = 1.0 / lmx, ily = 1.0 / lmy, igl = 1.0 / glz[z];
   const T* pu = unl + (size_t)z * plane;
   double mu = 0, mv = 0, mw = 0, ml = 0;
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < plane; i += (size_t)gridDim.x * blockDim.x) {
-    const double u = fabs((double)pu[i]), v = fabs((double)pu[P + i]), w = fabs((double)pu[2 * P + i]);
+  auto point = [&](T a, T b, T c) {
+    const double u = fabs((double)a), v = fabs((double)b), w = fabs((double)c);
     mu = max_keep_nan(mu, u);
     mv = max_keep_nan(mv, v);
     mw = max_keep_nan(mw, w);
     ml = max_keep_nan(ml, u * ilx + v * ily + w * igl);
+  };
+  const size_t t0 = blockIdx.x * (size_t)blockDim.x + threadIdx.x, step = (size_t)gridDim.x * blockDim.x;
+  // 16-byte vectors of the three fields (the maxima do not depend on the
+  // order), the plane's tail, if any, one value at a time
+  constexpr int EV = 16 / sizeof(T);
+  using V = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
+  const size_t nvec = (plane % EV == 0 && P % EV == 0) ? plane / EV : 0;
+  const V* pv = reinterpret_cast<const V*>(pu);
+  for (size_t i = t0; i < nvec; i += step) {
+    const V a = pv[i], b = pv[P / EV + i], c = pv[2 * P / EV + i];
+    const T* ta = reinterpret_cast<const T*>(&a);
+    const T* tb = reinterpret_cast<const T*>(&b);
+    const T* tc = reinterpret_cast<const T*>(&c);
+#pragma unroll
+    for (int e = 0; e < EV; ++e) point(ta[e], tb[e], tc[e]);
   }
+  for (size_t i = nvec * EV + t0; i < plane; i += step) point(pu[i], pu[P + i], pu[2 * P + i]);
   double mx[4] = {mu, mv, mw, ml};
 #pragma unroll
   for (int k = 0; k < 4; ++k)
