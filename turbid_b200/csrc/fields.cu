@@ -494,23 +494,38 @@ __device__ __forceinline__ void filter_classify(T x, double& sp, int& cp, double
   cn += d < 0 ? 1 : 0;
 }
 
-template <typename T>
+// W values per access: 16-byte vectors where the plane is a whole number of
+// them (W = 16 / sizeof(T)), one value otherwise; every thread keeps
+// kFilterBatch values of a sweep in flight either way
+template <typename T, int W>
+struct alignas(sizeof(T) * W) FilterVec {
+  T e[W];
+};
+
+template <typename T, int W>
 __global__ void __launch_bounds__(kFilterThreads, 2) k_filter(T* __restrict__ phip, int plane_n) {
-  constexpr int FB = kFilterBatch, STEP = FB * kFilterThreads;
+  using V = FilterVec<T, W>;
+  constexpr int FB = kFilterBatch / W, STEP = FB * kFilterThreads;
   __shared__ double red[4][32];
   __shared__ double tot[4];
-  T* p = phip + (size_t)blockIdx.x * plane_n;
+  V* p = reinterpret_cast<V*>(phip + (size_t)blockIdx.x * plane_n);
+  const int nv = plane_n / W;
   double sp = 0, sn = 0;
   int cp = 0, cn = 0;
-  for (int i0 = threadIdx.x; i0 < plane_n; i0 += STEP) {
-    T x[FB];
+  for (int i0 = threadIdx.x; i0 < nv; i0 += STEP) {
+    V x[FB];
 #pragma unroll
     for (int b = 0; b < FB; ++b) {
       const int i = i0 + b * kFilterThreads;
-      x[b] = i < plane_n ? p[i] : T(0);
+      if (i < nv) x[b] = p[i];
+      else
+#pragma unroll
+        for (int e = 0; e < W; ++e) x[b].e[e] = T(0);
     }
 #pragma unroll
-    for (int b = 0; b < FB; ++b) filter_classify(x[b], sp, cp, sn, cn);
+    for (int b = 0; b < FB; ++b)
+#pragma unroll
+      for (int e = 0; e < W; ++e) filter_classify(x[b].e[e], sp, cp, sn, cn);
   }
   for (int it = 0; it < 5; ++it) {
     double a[4] = {sp, (double)cp, sn, (double)cn};
@@ -519,19 +534,27 @@ __global__ void __launch_bounds__(kFilterThreads, 2) k_filter(T* __restrict__ ph
     const double add = tot[1] > 0 ? tot[2] / tot[1] : 0.0;
     sp = sn = 0;
     cp = cn = 0;
-    for (int i0 = threadIdx.x; i0 < plane_n; i0 += STEP) {
-      T x[FB];
+    for (int i0 = threadIdx.x; i0 < nv; i0 += STEP) {
+      V x[FB];
 #pragma unroll
       for (int b = 0; b < FB; ++b) {
         const int i = i0 + b * kFilterThreads;
-        x[b] = i < plane_n ? p[i] : T(0);
+        if (i < nv) x[b] = p[i];
+        else
+#pragma unroll
+          for (int e = 0; e < W; ++e) x[b].e[e] = T(0);
       }
 #pragma unroll
       for (int b = 0; b < FB; ++b) {
         const int i = i0 + b * kFilterThreads;
-        const T y = kill ? T(0) : ((x[b] > 0) ? (T)((double)x[b] + add) : T(0));
-        if (i < plane_n) p[i] = y;
-        filter_classify(y, sp, cp, sn, cn);   // sums for the next sweep
+        V y;
+#pragma unroll
+        for (int e = 0; e < W; ++e) {
+          const T v = x[b].e[e];
+          y.e[e] = kill ? T(0) : ((v > 0) ? (T)((double)v + add) : T(0));
+          filter_classify(y.e[e], sp, cp, sn, cn);   // sums for the next sweep
+        }
+        if (i < nv) p[i] = y;
       }
     }
     __syncthreads();   // the next sweep's reduction reuses red/tot
@@ -540,7 +563,11 @@ __global__ void __launch_bounds__(kFilterThreads, 2) k_filter(T* __restrict__ ph
 template <typename T>
 void positivity_filter(T* phip, int plane_n, int nz, cudaStream_t s) {
   prof_begin(s, PC_FILTER, 11.0 * sizeof(T) * (double)plane_n * nz, 0);   // 6 reads + 5 writes of the plane
-  k_filter<T><<<nz, kFilterThreads, 0, s>>>(phip, plane_n);
+  constexpr int W = 16 / sizeof(T);
+  if (plane_n % W == 0 && reinterpret_cast<uintptr_t>(phip) % 16 == 0)
+    k_filter<T, W><<<nz, kFilterThreads, 0, s>>>(phip, plane_n);
+  else
+    k_filter<T, 1><<<nz, kFilterThreads, 0, s>>>(phip, plane_n);
   prof_end(s);
   TG_LAUNCH_CHECK("k_filter");
 }
