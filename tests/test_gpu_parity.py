@@ -223,9 +223,12 @@ def test_fp64_steps_positivity_filter_active(cuda):
     _compare_run(cfg, 3, seed=13, noise=0.05, tol=1e-10, **filter_active_state_kw(cfg.nz))
 
 
-def test_mixed_positivity_filter_active_close_to_fp64(cuda):
-    """The FP32 filter of the mixed mode on the same zero-crossing scalar."""
-    cfg = sediment_cfg(nx=32, ny=32, nz=17)
+@pytest.mark.parametrize("nx,ny", [(32, 32), (30, 27)])
+def test_mixed_positivity_filter_active_close_to_fp64(cuda, nx, ny):
+    """The FP32 filter of the mixed mode on the same zero-crossing scalar;
+    30 x 27 = 810 points per plane is no whole number of four-value vectors,
+    so the filter and the feature reduction take their one-value path."""
+    cfg = sediment_cfg(nx=nx, ny=ny, nz=17)
     uvw, p, phi = O.make_initial_state(cfg, seed=13, noise=0.05, **filter_active_state_kw(cfg.nz))
     f64 = gpu_case(cfg, "fp64")
     mx = gpu_case(cfg, "mixed")
